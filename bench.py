@@ -1,0 +1,439 @@
+#!/usr/bin/env python
+"""bench.py -- 1080p Basic+Final Mpix/s of the plain FP32 path on B200.
+
+Workload (one step): 8 synthetic RGB float32 1920x1080 frames per GPU through
+    RGB2OPP(sample=1) -> Basic(profile='np', matrix=100) -> Final(ref=basic, profile='np',
+    matrix=100) -> OPP2RGB(sample=1), sigma 10,
+the full-pipeline configuration of the reference plugin's benchmark (8 frames, 1080p RGB).
+`value` times the device-resident pipeline (frames already in HBM); `e2e` times the same calls with
+pinned host frames (host->device and device->host copies inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: one process per GPU (torchrun), each rank processes its own 8 frames (frame sharding,
+no collective on the data path; weak scaling); barrier + max over ranks of the device time.
+--impl reference times the CPU oracle (the reference's path restated in C++; the reference plugin
+itself needs FFTW and VapourSynth, absent here) on the host cores.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "vapoursynth-bm3d_b200"))
+
+W, H, NFR, SIGMA = 1920, 1080, 8, 10.0
+METRIC = "1080p Basic+Final Mpix/s: plain FP32 vs TC+learned-BM form at ≤0.05 dB PSNR loss"
+WORKLOAD = "RGB float32 1920x1080 x8 frames/GPU: RGB2OPP(sample=1) -> Basic(np, matrix=100) -> Final(np, matrix=100, ref=basic) -> OPP2RGB(sample=1), sigma 10"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--frames", type=int, default=NFR)
+    ap.add_argument("--width", type=int, default=W)
+    ap.add_argument("--height", type=int, default=H)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ---- CPU side (oracle) ---------------------------------------------------------------------------
+
+def cpu_sample(threads, frames, width, rows):
+    """Times the CPU oracle on `threads` frames cropped to `rows` rows (one frame per thread, as
+    VapourSynth's fmParallel does).  Returns (Mpix/s, seconds, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    from bm3d_b200 import synth
+    nz, _ = synth.rgb_frames(1, frames, rows, width, SIGMA)
+    t0 = time.perf_counter()
+    opp = np.stack([oracle.rgb2opp(nz[k]) for k in range(frames)])
+    pb = oracle.default_params(0, False, "np", SIGMA, matrix=100)
+    basic = oracle.bm3d(pb, opp, threads=threads)
+    pf = oracle.default_params(1, False, "np", SIGMA, matrix=100)
+    final = oracle.bm3d(pf, opp, basic, threads=threads)
+    _ = [oracle.opp2rgb(final[k]) for k in range(frames)]
+    dt = time.perf_counter() - t0
+    mpix = frames * width * rows / dt / 1e6
+    return mpix, dt, f"{frames} frame crops of {width}x{rows} (rows 0..{rows - 1} of the config frames), one per thread"
+
+
+def reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    threads = min(os.cpu_count() or 1, args.frames)
+    rows = 136
+    vals = []
+    for i in range(args.warmup + args.steps):
+        mpix, dt, sample = cpu_sample(threads, threads, args.width, rows)
+        if i >= args.warmup:
+            vals.append((mpix, dt))
+    value = statistics.median(v[0] for v in vals)
+    ms = statistics.median(v[1] for v in vals) * 1e3
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mpix/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "frames_per_gpu": args.frames, "width": args.width, "height": args.height},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mpix/s", "cores": threads, "kind": "port",
+                         "sample": sample + "; CPU oracle (bm3d_oracle.cpp) restating the reference's path, "
+                                            "FFTW replaced by a separable FP32 DCT"},
+        "e2e": {"value": round(value, 4), "unit": "Mpix/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- GPU side ----------------------------------------------------------------------------------
+
+class Clocks:
+    """Samples nvidia-smi during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def fp32_peak_tflops(torch):
+    """Measured FP32 (no TF32) cuBLAS SGEMM throughput on this GPU: the SIMT FP32 ceiling."""
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    b = torch.randn(n, n, device="cuda", dtype=torch.float32)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def scan(extent, B, step):
+    out, j, last = [], 0, extent - B
+    while True:
+        if j >= last + step:
+            break
+        if j > last:
+            j = last
+        out.append(j)
+        j += step
+    return out
+
+
+def lattice_count(pos, lim, rng):
+    lo = max(0, pos - rng)
+    hi = min(lim, pos + rng)
+    return hi - lo + 1
+
+
+def algorithmic_work(width, height, frames, step, G, n_mean, wiener):
+    """SURVEY-style algorithmic FLOPs of one call: BM = 3*B^2 per evaluated candidate (sub, mul,
+    add per pixel); DCT = dense separable count 2*(n*2B^3 + B^2*n^2) per transform, 2 transforms
+    (Basic) or 3 (Final) per group and plane, 3 planes."""
+    B, R = 8, 16
+    ys, xs = scan(height, B, step), scan(width, B, step)
+    cy = sum(lattice_count(y, height - B, R) for y in ys)
+    cx = sum(lattice_count(x, width - B, R) for x in xs)
+    cands = cy * cx                     # lattice minus self plus the trailing (0,0) candidate
+    bm = 3.0 * B * B * cands * frames
+    ng = len(ys) * len(xs) * frames
+    n = n_mean
+    dct = 2.0 * (n * 2 * B ** 3 + B * B * n * n) * (3 if wiener else 2) * 3 * ng
+    return bm, dct, ng
+
+
+class Stage:
+    def __init__(self, L, name, args, inputs):
+        from bm3d_b200 import _capi as capi
+        m = L.bm3d_map_create()
+        for k, v in args.items():
+            if isinstance(v, capi.VideoInfo):
+                L.bm3d_map_set_clip(m, k.encode(), C.byref(v))
+            elif isinstance(v, str):
+                L.bm3d_map_set_data(m, k.encode(), v.encode())
+            elif isinstance(v, float):
+                L.bm3d_map_set_float(m, k.encode(), v)
+            else:
+                L.bm3d_map_set_int(m, k.encode(), v)
+        self.h = C.c_void_p()
+        rc = L.bm3d_create(name.encode(), m, C.byref(self.h))
+        L.bm3d_map_free(m)
+        if rc:
+            raise RuntimeError(capi.last_error())
+        self.info = capi.VideoInfo()
+        L.bm3d_output_info(self.h, C.byref(self.info))
+
+
+def make_frames(capi, planes, memory):
+    PF = C.POINTER(capi.Frame)
+    structs = []
+    for pl in planes:
+        fr = capi.Frame()
+        for p, a in enumerate(pl):
+            if memory == capi.MEM_DEVICE:
+                fr.data[p] = a.data_ptr()
+                fr.stride[p] = a.stride(0) * a.element_size()
+            else:
+                fr.data[p] = a.data_ptr()
+                fr.stride[p] = a.stride(0) * a.element_size()
+        fr.memory = memory
+        fr.prop_bm3d_opp = fr.prop_range = fr.prop_matrix = fr.prop_v_radius = -1
+        fr.prop_v_process_count = -1
+        structs.append(fr)
+    arr = (PF * len(structs))(*[C.pointer(s) for s in structs])
+    return structs, arr
+
+
+def ours_arm(args):
+    import numpy as np
+    import torch
+    from bm3d_b200 import _capi as capi
+    from bm3d_b200 import synth
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as tdist
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+
+    L = capi.lib()
+    F, Wd, Hd = args.frames, args.width, args.height
+    # synthetic frames: each rank its own seeds (frame sharding)
+    nz, clean = synth.rgb_frames(1 + rank, F, Hd, Wd, SIGMA)
+    rgb_in = torch.from_numpy(nz).cuda()
+    stream = torch.cuda.Stream()
+    vi = capi.VideoInfo(capi.RGB, capi.FLOAT, 32, 0, 0, Wd, Hd, F)
+    s_opp = Stage(L, "RGB2OPP", {"input": vi, "sample": 1}, None)
+    s_basic = Stage(L, "Basic", {"input": s_opp.info, "profile": "np", "matrix": 100, "sigma": SIGMA}, None)
+    s_final = Stage(L, "Final", {"input": s_opp.info, "ref": s_basic.info, "profile": "np", "matrix": 100, "sigma": SIGMA}, None)
+    s_rgb = Stage(L, "OPP2RGB", {"input": s_final.info, "sample": 1}, None)
+    for s in (s_opp, s_basic, s_final, s_rgb):
+        L.bm3d_set_stream(s.h, C.c_void_p(stream.cuda_stream))
+
+    def planes(n):
+        return [[torch.empty((Hd, Wd), dtype=torch.float32, device="cuda") for _ in range(3)] for _ in range(n)]
+
+    f_in = [[rgb_in[k, p] for p in range(3)] for k in range(F)]
+    f_opp, f_basic, f_final, f_out = planes(F), planes(F), planes(F), planes(F)
+    D = capi.MEM_DEVICE
+    _, a_in = make_frames(capi, f_in, D)
+    _, a_opp = make_frames(capi, f_opp, D)
+    _, a_basic = make_frames(capi, f_basic, D)
+    _, a_final = make_frames(capi, f_final, D)
+    _, a_out = make_frames(capi, f_out, D)
+
+    def step_device():
+        for (s, src, ref, dst) in ((s_opp, a_in, None, a_opp), (s_basic, a_opp, None, a_basic),
+                                   (s_final, a_opp, a_basic, a_final), (s_rgb, a_final, None, a_out)):
+            if L.bm3d_get_frames_async(s.h, 0, F, src, ref, dst) != 0:
+                raise RuntimeError(capi.last_error())
+
+    # host (pinned) frames for the end-to-end measurement
+    h_in = torch.from_numpy(nz).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    H_ = capi.MEM_HOST
+    _, ah_in = make_frames(capi, [[h_in[k, p] for p in range(3)] for k in range(F)], H_)
+    _, ah_out = make_frames(capi, [[h_out[k, p] for p in range(3)] for k in range(F)], H_)
+
+    def step_e2e():
+        for (s, src, ref, dst) in ((s_opp, ah_in, None, a_opp), (s_basic, a_opp, None, a_basic),
+                                   (s_final, a_opp, a_basic, a_final), (s_rgb, a_final, None, ah_out)):
+            if L.bm3d_get_frames_async(s.h, 0, F, src, ref, dst) != 0:
+                raise RuntimeError(capi.last_error())
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(fn, steps, warmup, profile=False):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        if profile:
+            for s in (s_basic, s_final):
+                L.bm3d_set_profiling(s.h, 1)
+        stage = {"basic": [0.0] * 6, "final": [0.0] * 6}
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        total = 0.0
+        launches0 = L.bm3d_debug_launch_count()
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+            fn()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+            if profile:
+                buf = (C.c_double * 6)()
+                for name, s in (("basic", s_basic), ("final", s_final)):
+                    if L.bm3d_debug_stage_times(s.h, buf, 6) == 6:
+                        for i in range(6):
+                            stage[name][i] += buf[i]
+        launches = L.bm3d_debug_launch_count() - launches0
+        barrier()
+        if profile:
+            for s in (s_basic, s_final):
+                L.bm3d_set_profiling(s.h, 0)
+        ms = total / steps
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, {k: [v / steps for v in vs] for k, vs in stage.items()}, launches // steps
+
+    peak = fp32_peak_tflops(torch) if rank == 0 else None
+    clocks = Clocks(local)
+    clocks.start()
+    ms, stage, launches = timed(step_device, args.steps, args.warmup, profile=True)
+    clk = clocks.stop()
+    ms_plain, _, _ = timed(step_device, args.steps, 1, profile=False)
+    ms_e2e, _, _ = timed(step_e2e, args.steps, args.warmup, profile=False)
+
+    # quality check of the timed output against the clean frames (PSNR)
+    out = torch.stack([torch.stack(f) for f in f_out]).cpu().numpy()
+    mse = float(np.mean((out - clean) ** 2))
+    psnr = 10 * np.log10(1.0 / mse)
+    mse_in = float(np.mean((nz - clean) ** 2))
+    psnr_in = 10 * np.log10(1.0 / mse_in)
+
+    # group fill of frame 0 (mean n) for the algorithmic work count
+    nb_b = len(scan(Hd, 8, 4)) * len(scan(Wd, 8, 4))
+    nb_f = len(scan(Hd, 8, 3)) * len(scan(Wd, 8, 3))
+
+    def mean_n(s, G, nb):
+        cnt = np.zeros(nb, np.int32)
+        z = np.zeros(nb * G, np.int32)
+        P = C.POINTER
+        rc = L.bm3d_debug_matches(s.h, 0, cnt.ctypes.data_as(P(C.c_int)), z.ctypes.data_as(P(C.c_int)),
+                                  z.ctypes.data_as(P(C.c_int)), z.ctypes.data_as(P(C.c_int)),
+                                  np.zeros(nb * G, np.float32).ctypes.data_as(P(C.c_float)), nb)
+        return float(cnt.mean()) if rc > 0 else float(G)
+
+    nb_mean, nf_mean = mean_n(s_basic, 16, nb_b), mean_n(s_final, 32, nb_f)
+    bm_b, dct_b, _ = algorithmic_work(Wd, Hd, F, 4, 16, nb_mean, False)
+    bm_f, dct_f, _ = algorithmic_work(Wd, Hd, F, 3, 32, nf_mean, True)
+    cands = {
+        "basic_block_matching": (stage["basic"][1], bm_b),
+        "basic_collaborative_filter": (stage["basic"][3], dct_b),
+        "final_block_matching": (stage["final"][1], bm_f),
+        "final_collaborative_filter": (stage["final"][3], dct_f),
+    }
+    dom = max(cands, key=lambda k: cands[k][0])
+    t_dom, w_dom = cands[dom]
+
+    if rank == 0:
+        value = F * Wd * Hd * world / (ms * 1e-3) / 1e6
+        v_e2e = F * Wd * Hd * world / (ms_e2e * 1e-3) / 1e6
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            try:
+                traffic = json.load(open(tpath)).get(dom)
+            except Exception:
+                traffic = None
+        achieved = w_dom / (t_dom * 1e-3) / 1e12 if t_dom > 0 else None
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mpix/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "frames_per_gpu": F, "width": Wd, "height": Hd,
+                       "parallelism": f"frame-sharded replicas x{world}",
+                       "l2": "inputs larger than L2 (199 MB of input frames, ~2 GB working set per step)"},
+            "roofline": {"bound": "fp32", "kernel": dom, "achieved": round(achieved, 3) if achieved else None,
+                         "peak": round(peak, 3) if peak else None, "unit": "TFLOP/s",
+                         "frac": round(achieved / peak, 4) if (achieved and peak) else None, "traffic": traffic,
+                         "peak_source": "measured in-process: cuBLAS SGEMM FP32 (TF32 off), 8192^3 best of 5",
+                         "work": "SURVEY 8(d) algorithmic FLOPs: BM 3*B^2 per candidate; DCT 2*(n*2B^3+B^2*n^2) per transform"},
+            "stages_ms": {"basic": [round(v, 3) for v in stage["basic"]], "final": [round(v, 3) for v in stage["final"]],
+                          "order": ["ingest", "block_matching", "predictive", "collaborative_filter", "normalise", "egress"]},
+            "e2e": {"value": round(v_e2e, 3), "unit": "Mpix/s", "h2d_bytes_per_step": int(nz.nbytes),
+                    "d2h_bytes_per_step": int(nz.nbytes), "ms_per_step": round(ms_e2e, 3)},
+            "ms_per_step_unprofiled": round(ms_plain, 3),
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "quality": {"psnr_in_db": round(psnr_in, 3), "psnr_out_db": round(psnr, 3)},
+        }
+        if not args.no_cpu_baseline:
+            threads = min(os.cpu_count() or 1, F)
+            mpix, dt, sample = cpu_sample(threads, threads, Wd, 136)
+            line["cpu_baseline"] = {"value": round(mpix, 4), "unit": "Mpix/s", "cores": threads, "kind": "port",
+                                    "sample": sample, "seconds": round(dt, 2)}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        ours_arm(args)
+
+
+if __name__ == "__main__":
+    main()

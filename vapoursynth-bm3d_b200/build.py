@@ -1,0 +1,50 @@
+"""Build recipe for the in-tree shared library lib/libbm3d_b200.so (sm_100a).
+
+Compiles csrc/kernels.cu (every kernel) and csrc/host.cpp (argument processing, filter objects,
+C ABI of include/bm3d_b200.h) with nvcc, linking the CUDA runtime statically so the library only
+needs the NVIDIA driver at run time.
+"""
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB_DIR = os.path.join(HERE, "lib")
+LIB = os.path.join(LIB_DIR, "libbm3d_b200.so")
+SOURCES = ["kernels.cu", "host.cpp"]
+DEPS = SOURCES + ["args.h", "bm.cuh", "cf.cuh", "common.cuh", "convert.cuh", "launch.h", "params.h",
+                  "select.cuh", "vbm.cuh", os.path.join("..", "..", "include", "bm3d_b200.h")]
+
+
+def nvcc_path():
+    for cand in (shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def needs_build():
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(os.path.join(CSRC, d)) > t for d in DEPS)
+
+
+def build(force=False, verbose=False):
+    if not force and not needs_build():
+        return LIB
+    os.makedirs(LIB_DIR, exist_ok=True)
+    cmd = [nvcc_path(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+           "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared", "-cudart", "static",
+           "-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True, cwd=CSRC)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose=True))

@@ -1,0 +1,184 @@
+// args.h -- plain argument structures shared by the host code and the kernels (no device code).
+#pragma once
+
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define BM3D_HD __host__ __device__
+#else
+#define BM3D_HD
+#endif
+
+namespace bm3d {
+
+// ---------------------------------------------------------------------------------------------
+// Packed block positions.  BM3D lists: (y << 16) | x.  V-BM3D lists: (z << 26) | (y << 13) | x
+// with z the frame index inside the temporal window (< 64) and y, x < 8192.
+
+BM3D_HD inline uint32_t pack_yx(int y, int x) { return ((uint32_t)y << 16) | (uint32_t)x; }
+BM3D_HD inline int unpack_y(uint32_t p) { return (int)(p >> 16); }
+BM3D_HD inline int unpack_x(uint32_t p) { return (int)(p & 0xffffu); }
+
+BM3D_HD inline uint32_t pack_zyx(int z, int y, int x) { return ((uint32_t)z << 26) | ((uint32_t)y << 13) | (uint32_t)x; }
+BM3D_HD inline int unpack3_z(uint32_t p) { return (int)(p >> 26); }
+BM3D_HD inline int unpack3_y(uint32_t p) { return (int)((p >> 13) & 0x1fffu); }
+BM3D_HD inline int unpack3_x(uint32_t p) { return (int)(p & 0x1fffu); }
+
+// Shared-memory floats per warp (host and device must agree).
+BM3D_HD inline int bm_warp_floats(int cand_cap, int G, int B, bool generic)
+{
+    return cand_cap + 64 + 2 * G + (generic ? B * B : 0);
+}
+BM3D_HD inline int vbm_warp_floats(int sp_cap, int list_cap, int G, int ps_num, int B)
+{
+    return 3 * sp_cap + 4 * list_cap + 2 * G + ps_num + B * B;
+}
+
+enum SampleKind : int { SK_U8 = 0, SK_U16 = 1, SK_F32 = 2 };
+
+struct BMArgs {
+    const float *ref;          // plane of frame 0; frame f at ref + f * frame_stride
+    long long frame_stride;
+    int ld, H, W;
+    int B, range, step;        // range already rounded down to a multiple of step
+    int G;
+    float thSSE;
+    double distMul;
+    const int *scan_y;
+    const int *scan_x;
+    int nby, nbx;
+    uint32_t *out_pos;         // [frame][by][bx][G], packed (y << 16) | x
+    int *out_n;                // [frame][by][bx]
+    float *out_key;            // optional, [frame][by][bx][G]
+    unsigned long long *stats; // optional: [0] blocks that took the exact heap path
+    int warps;                 // warps per CTA
+    int win_h, win_pitch;      // shared window capacity
+    int cand_cap;              // per-warp distance slots (>= lattice + 1)
+};
+
+struct CFArgs {
+    // planes of frame 0 (float workspace), frame f at + f * frame_stride
+    const float *src[3];
+    const float *ref[3];
+    float *num[3];
+    float *wmap[3];
+    long long frame_stride;
+    int ld, H, W;
+    int process[3];
+    int B, G;
+    int wiener;
+    // match lists: groups ordered [frame][by][bx]; blocks_per_frame = nby * nbx
+    const uint32_t *pos;       // [group][G], packed (y<<16)|x, or (z<<26)|(y<<13)|x for V-BM3D
+    const int *count;          // [group]
+    long long ngroups;
+    long long blocks_per_frame;
+    int vbm3d;                 // positions carry a window frame index
+    // V-BM3D: planes of window frame z for output frame f are at src[p] + (win_base[f] + z) *
+    // frame_stride; accumulator slot for window frame z at num[p] + (f * slots + slot0[f] + z) * acc_stride
+    const int *win_base;       // [frame] first clip frame of the window (V-BM3D)
+    const int *slot0;          // [frame] first slot index (V-BM3D)
+    int slots;                 // slots per output frame (2r+1)
+    long long acc_stride;      // elements between accumulator slots
+    // filter data per plane
+    float thr4[3][256][4];     // [plane][n-1][flag]   (Basic)
+    float wsig2[3][256];       // [plane][n-1]         (Final)
+    float amp[256];            // finalAMP[n-1] = 2n*2B*2B (exact in float)
+    // generic path
+    const float *odd_all;      // odd tables N = 2..256
+    const float *dtab;         // direct tables (fwd then inv) for non-power-of-two N
+    const int *dtab_off;       // [N] offset of the fwd table of length N in dtab (-1 if absent)
+    float *scratch;            // per-warp scratch for the generic path
+    long long scratch_per_warp;
+    int skip_full;             // generic kernel: skip groups the fast kernel handles
+};
+
+struct VBMArgs {
+    const float *ref;             // reference Y planes of the clip window workspace
+    long long frame_stride;
+    int ld, H, W;
+    int B, G, ps_num, ps_range, ps_step;   // ps_range already rounded to a multiple of ps_step
+    float thSSE;
+    double distMul;
+    const int *scan_y, *scan_x;
+    int nby, nbx;
+    // per output frame f of the batch: window start (clip frame index in the workspace), length,
+    // index of the current frame inside the window
+    const int *win_base, *win_len, *win_cur;
+    // current-frame lists from K1: [f][by][bx][G] positions (y<<16|x), keys, counts
+    const uint32_t *cur_pos;
+    const float *cur_key;
+    const int *cur_n;
+    // output: [f][by][bx][G] packed (z<<26|y<<13|x), optional keys, counts
+    uint32_t *out_pos;
+    float *out_key;
+    int *out_n;
+    unsigned long long *stats;
+    int warps;
+    int sp_cap;                   // capacity of the per-warp search-position list
+    int list_cap;                 // capacity of the per-warp concatenated list
+};
+
+struct PlanePtr {
+    void *ptr;
+    long long stride;   // bytes
+};
+
+// One linear channel: out = clip?(in * gain + offset)
+struct LinearOp {
+    float gain, offset, lo, hi;
+    int clip;
+};
+
+// Conversion program for one frame set.  mode:
+//   0 LINEAR  : out[c] = op[c](in[c])                       (RangeConvert)
+//   1 RGB2OPP : Y = ((R+G)+B)*gY+oY, U = (R-B)*gU+oC, V = ((R-2G)+B)*gV+oC   (MatrixConvert_RGB2YUV)
+//   2 RGB2Y   : Y = ((R+G)+B)*g+o                               (ConvertToY, OPP)
+//   3 OPP2RGB : R = ((Ry*Y+Ru*U)+Rv*V)+oR, G = (Gy*Y+Gv*V)+oG, B = ((By*Y+Bu*U)+Bv*V)+oB
+struct ConvProgram {
+    int mode;
+    int raw;                // 1: plain copy (same sample kind in and out)
+    int in_kind, out_kind;
+    int nin, nout;
+    LinearOp op[3];
+    float coef[9];          // OPP2RGB: Ry Ru Rv Gy Gu Gv By Bu Bv (already scaled by the gains)
+    float off[3];
+    int W, H;
+};
+
+// finalize: out = num / box_B(wmap) for processed planes of a batch of frames.
+struct FinalizeArgs {
+    const float *num[3];
+    const float *wmap[3];
+    float *out[3];
+    long long frame_stride;
+    int ld, H, W, B;
+    int process[3];
+};
+
+// VAggregate for a batch of output frames.  in[(f * frames_max + i) * 3 + p] points to plane p of
+// the stacked frame n + b_off + i; slot o = radius - b_off - i holds the numerator, o + 1 the
+// denominator.  The result is written as float into out workspace planes.
+struct VAggArgs {
+    const PlanePtr *in;
+    int frames_max;
+    const int *nframes;     // [f] window length
+    const int *b_off;       // [f]
+    float *out[3];
+    long long frame_stride;
+    int ld, H, W, radius;
+    int process[3];
+};
+
+// V-BM3D output: per output frame f and window slot s, writes the numerator plane (slot 2s) and
+// the denominator plane (slot 2s+1, the B x B box sum of the per-origin weights) into the
+// stacked float frame (height H * slots * 2).
+struct VStackArgs {
+    const float *num[3];
+    const float *wmap[3];
+    long long slot_stride;     // elements between accumulator slots
+    int ld, H, W, B, slots;
+    int process[3];
+    const PlanePtr *out;       // [f * 3 + p]
+};
+
+}  // namespace bm3d

@@ -1,0 +1,215 @@
+// kernels.cu -- the single CUDA translation unit holding every sm_100a kernel of the library
+// (block matching, predictive search, collaborative filter, conversions) and their launchers.
+
+#include "common.cuh"
+#include "select.cuh"
+#include "bm.cuh"
+#include "vbm.cuh"
+#include "cf.cuh"
+#include "convert.cuh"
+#include "launch.h"
+
+#include <atomic>
+
+namespace bm3d {
+
+// Every kernel launch of the library goes through a launcher below and is counted here.
+static std::atomic<unsigned long long> g_launches{0};
+unsigned long long launch_count() { return g_launches.load(); }
+#define COUNT_LAUNCH() g_launches.fetch_add(1, std::memory_order_relaxed)
+
+cudaError_t upload_odd_tables(const float *host_odd_all)
+{
+    return cudaMemcpyToSymbol(c_odd, host_odd_all, sizeof(float) * kOddConstFloats);
+}
+
+template <typename K>
+static cudaError_t allow_smem(K kernel, size_t bytes)
+{
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t launch_bm_full(const BMArgs &a, int nframes, size_t smem, cudaStream_t s)
+{
+    dim3 grid((a.nbx + a.warps - 1) / a.warps, a.nby, nframes);
+    dim3 block(32 * a.warps);
+    cudaError_t e;
+    if (a.B == 8) {
+        if ((e = allow_smem(bm_full_kernel<8>, smem)) != cudaSuccess) return e;
+        COUNT_LAUNCH();
+        bm_full_kernel<8><<<grid, block, smem, s>>>(a);
+    } else {
+        if ((e = allow_smem(bm_full_kernel<0>, smem)) != cudaSuccess) return e;
+        COUNT_LAUNCH();
+        bm_full_kernel<0><<<grid, block, smem, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vbm_predict(const VBMArgs &a, int nframes, size_t smem, cudaStream_t s)
+{
+    dim3 grid((a.nbx + a.warps - 1) / a.warps, a.nby, nframes);
+    dim3 block(32 * a.warps);
+    cudaError_t e;
+    if ((e = allow_smem(vbm_predict_kernel, smem)) != cudaSuccess) return e;
+    COUNT_LAUNCH();
+    vbm_predict_kernel<<<grid, block, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+int cf_fast_supported(int B, int G) { return B == 8 && (G == 8 || G == 16 || G == 32); }
+
+template <int G, bool W>
+static cudaError_t launch_cf_fast_t(const CFArgs &a, int warps, int grid, cudaStream_t s)
+{
+    const size_t smem = (size_t)warps * (W ? 2 : 1) * 32 * 65 * sizeof(float);
+    cudaError_t e;
+    if ((e = allow_smem(cf_fast_kernel<G, W>, smem)) != cudaSuccess) return e;
+    COUNT_LAUNCH();
+    cf_fast_kernel<G, W><<<grid, 32 * warps, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cf_fast(const CFArgs &a, int warps, int grid, cudaStream_t s)
+{
+    if (a.B != 8) return cudaErrorInvalidValue;
+    const bool w = a.wiener != 0;
+    switch (a.G) {
+    case 8: return w ? launch_cf_fast_t<8, true>(a, warps, grid, s) : launch_cf_fast_t<8, false>(a, warps, grid, s);
+    case 16: return w ? launch_cf_fast_t<16, true>(a, warps, grid, s) : launch_cf_fast_t<16, false>(a, warps, grid, s);
+    case 32: return w ? launch_cf_fast_t<32, true>(a, warps, grid, s) : launch_cf_fast_t<32, false>(a, warps, grid, s);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_cf_generic(const CFArgs &a, int warps, int grid, cudaStream_t s)
+{
+    COUNT_LAUNCH();
+    cf_generic_kernel<<<grid, 32 * warps, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert(const ConvProgram &pr, const PlanePtr *in, const PlanePtr *out, int nframes,
+                           cudaStream_t s)
+{
+    dim3 block(256);
+    dim3 grid((pr.W + 255) / 256, pr.H, nframes);
+    COUNT_LAUNCH();
+    convert_kernel<<<grid, block, 0, s>>>(pr, in, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const FinalizeArgs &a, int nframes, cudaStream_t s)
+{
+    dim3 block(256);
+    dim3 grid((a.W + 255) / 256, a.H * 3, nframes);
+    COUNT_LAUNCH();
+    finalize_kernel<<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vaggregate(const VAggArgs &a, int nframes, cudaStream_t s)
+{
+    dim3 block(256);
+    dim3 grid((a.W + 255) / 256, a.H * 3, nframes);
+    COUNT_LAUNCH();
+    vaggregate_kernel<<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vstack(const VStackArgs &a, int nframes, cudaStream_t s)
+{
+    dim3 block(256);
+    dim3 grid((a.W + 255) / 256, a.H * a.slots, nframes * 3);
+    COUNT_LAUNCH();
+    vstack_kernel<<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+// ---- transform-only test kernels ------------------------------------------------------------
+
+template <int G>
+__global__ void dct_fast_test_kernel(float *data, int inverse)
+{
+    __shared__ float T[32 * 65];
+    const int lane = threadIdx.x;
+    float *g = data + (long long)blockIdx.x * G * 64;
+    constexpr int C = 64 / G;
+    if (!inverse) {
+        if (lane < G) {
+            float blk[64];
+#pragma unroll
+            for (int e = 0; e < 64; ++e) blk[e] = g[lane * 64 + e];
+            fwd2d8(blk);
+#pragma unroll
+            for (int e = 0; e < 64; ++e) T[lane * 65 + e] = blk[e];
+        }
+        __syncwarp();
+        if (lane < G) {
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                const int c = lane + q * G;
+                float col[G], X[G];
+#pragma unroll
+                for (int zz = 0; zz < G; ++zz) col[zz] = T[zz * 65 + c];
+                fdct_reg<G>(col, X);
+#pragma unroll
+                for (int zz = 0; zz < G; ++zz) g[zz * 64 + c] = X[zz];
+            }
+        }
+    } else {
+        if (lane < G) {
+#pragma unroll
+            for (int q = 0; q < C; ++q) {
+                const int c = lane + q * G;
+                float col[G], X[G];
+#pragma unroll
+                for (int zz = 0; zz < G; ++zz) X[zz] = g[zz * 64 + c];
+                idct_reg<G>(X, col);
+#pragma unroll
+                for (int zz = 0; zz < G; ++zz) T[zz * 65 + c] = col[zz];
+            }
+        }
+        __syncwarp();
+        if (lane < G) {
+            float blk[64];
+#pragma unroll
+            for (int e = 0; e < 64; ++e) blk[e] = T[lane * 65 + e];
+            inv2d8(blk);
+#pragma unroll
+            for (int e = 0; e < 64; ++e) g[lane * 64 + e] = blk[e];
+        }
+    }
+}
+
+__global__ void dct_generic_test_kernel(float *data, int n, int B, int inverse, CFArgs a)
+{
+    float tmp[512];
+    float *g = data + (long long)blockIdx.x * n * B * B;
+    dct3d_warp(g, n, B, inverse != 0, a, tmp);
+}
+
+cudaError_t launch_dct3d_test(float *data, int ngroups, int n, int B, int inverse, int fast,
+                              const float *odd_all, const float *dtab, const int *dtab_off,
+                              cudaStream_t s)
+{
+    if (fast) {
+        if (B != 8) return cudaErrorInvalidValue;
+        switch (n) {
+        case 8: dct_fast_test_kernel<8><<<ngroups, 32, 0, s>>>(data, inverse); break;
+        case 16: dct_fast_test_kernel<16><<<ngroups, 32, 0, s>>>(data, inverse); break;
+        case 32: dct_fast_test_kernel<32><<<ngroups, 32, 0, s>>>(data, inverse); break;
+        default: return cudaErrorInvalidValue;
+        }
+    } else {
+        CFArgs a{};
+        a.odd_all = odd_all;
+        a.dtab = dtab;
+        a.dtab_off = dtab_off;
+        dct_generic_test_kernel<<<ngroups, 32, 0, s>>>(data, n, B, inverse, a);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace bm3d

@@ -1,0 +1,36 @@
+// launch.h -- host-side entry points of the kernel translation unit (kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include "args.h"
+
+namespace bm3d {
+
+// Copies the odd-part DCT tables for N = 2..64 into constant memory of the current device.
+cudaError_t upload_odd_tables(const float *host_odd_all);
+
+cudaError_t launch_bm_full(const BMArgs &a, int nframes, size_t smem_bytes, cudaStream_t s);
+cudaError_t launch_vbm_predict(const VBMArgs &a, int nframes, size_t smem_bytes, cudaStream_t s);
+// Fast collaborative filter (B = 8, full groups, G in {8, 16, 32}); returns cudaErrorInvalidValue
+// for other shapes.
+cudaError_t launch_cf_fast(const CFArgs &a, int warps, int grid, cudaStream_t s);
+cudaError_t launch_cf_generic(const CFArgs &a, int warps, int grid, cudaStream_t s);
+cudaError_t launch_convert(const ConvProgram &pr, const PlanePtr *in_dev, const PlanePtr *out_dev,
+                           int nframes, cudaStream_t s);
+cudaError_t launch_finalize(const FinalizeArgs &a, int nframes, cudaStream_t s);
+cudaError_t launch_vaggregate(const VAggArgs &a, int nframes, cudaStream_t s);
+cudaError_t launch_vstack(const VStackArgs &a, int nframes, cudaStream_t s);
+
+// Transform-only entry points used by the bit-exactness tests: ngroups groups of n blocks of
+// B x B floats (layout [group][z][y][x]) transformed in place.  fast selects the register path
+// (B = 8, n in {8, 16, 32}).
+cudaError_t launch_dct3d_test(float *data, int ngroups, int n, int B, int inverse, int fast,
+                              const float *odd_all, const float *dtab, const int *dtab_off,
+                              cudaStream_t s);
+
+int cf_fast_supported(int B, int G);
+
+// Number of kernels launched by this library since load.
+unsigned long long launch_count();
+
+}  // namespace bm3d

@@ -370,9 +370,11 @@ def ours_arm(args):
         rc = L.bm3d_debug_matches(s.h, 0, cnt.ctypes.data_as(P(C.c_int)), z.ctypes.data_as(P(C.c_int)),
                                   z.ctypes.data_as(P(C.c_int)), z.ctypes.data_as(P(C.c_int)),
                                   np.zeros(nb * G, np.float32).ctypes.data_as(P(C.c_float)), nb)
-        return float(cnt.mean()) if rc > 0 else float(G)
+        if rc <= 0:
+            return float(G), 1.0
+        return float(cnt.mean()), float((cnt == G).mean())
 
-    nb_mean, nf_mean = mean_n(s_basic, 16, nb_b), mean_n(s_final, 32, nb_f)
+    (nb_mean, nb_full), (nf_mean, nf_full) = mean_n(s_basic, 16, nb_b), mean_n(s_final, 32, nb_f)
     bm_b, dct_b, _ = algorithmic_work(Wd, Hd, F, 4, 16, nb_mean, False)
     bm_f, dct_f, _ = algorithmic_work(Wd, Hd, F, 3, 32, nf_mean, True)
     cands = {
@@ -412,6 +414,8 @@ def ours_arm(args):
             "e2e": {"value": round(v_e2e, 3), "unit": "Mpix/s", "h2d_bytes_per_step": int(nz.nbytes),
                     "d2h_bytes_per_step": int(nz.nbytes), "ms_per_step": round(ms_e2e, 3)},
             "ms_per_step_unprofiled": round(ms_plain, 3),
+            "groups": {"basic_mean_n": round(nb_mean, 3), "basic_full_fraction": round(nb_full, 4),
+                       "final_mean_n": round(nf_mean, 3), "final_full_fraction": round(nf_full, 4)},
             "gpu_launches": int(launches),
             "clocks": clk,
             "quality": {"psnr_in_db": round(psnr_in, 3), "psnr_out_db": round(psnr, 3)},

@@ -313,8 +313,9 @@ static void dct1d(float *data, int N, ptrdiff_t stride, bool inverse)
 }
 
 // Group layout: data[(z*B + y)*B + x] (BlockGroup, include/Block.h:1028-1029).
-// Forward: x, then y, then z.  Inverse: z, then y, then x.
-static void dct3d(float *g, int n, int B, bool inverse)
+// Forward: x, then y, then z.  Inverse: z, then y, then x.  (Scalar form; dct3d below computes
+// the same operation sequence on 8 columns at a time.)
+static void dct3d_scalar(float *g, int n, int B, bool inverse)
 {
     const ptrdiff_t plane = (ptrdiff_t)B * B;
     if (!inverse) {
@@ -330,6 +331,128 @@ static void dct3d(float *g, int n, int B, bool inverse)
         for (int z = 0; z < n; ++z)
             for (int y = 0; y < B; ++y) dct1d(g + z * plane + y * B, B, 1, true);
     }
+}
+
+// ---- the same transforms on VL independent columns at once -------------------------------------
+// Arrays are [index][lane]; every lane performs exactly the scalar operation sequence above, so
+// results are bit-identical (the lane loops only let the compiler use SIMD registers).
+constexpr int VL = 8;
+
+static void fdct_pow2_v(const float *x, int N, float *X)
+{
+    if (N == 1) {
+        for (int l = 0; l < VL; ++l) X[l] = x[l] * 2.0f;
+        return;
+    }
+    const int h = N / 2;
+    alignas(32) float e[128 * VL], o[128 * VL], E[128 * VL];
+    for (int j = 0; j < h; ++j)
+        for (int l = 0; l < VL; ++l) {
+            e[j * VL + l] = x[j * VL + l] + x[(N - 1 - j) * VL + l];
+            o[j * VL + l] = x[j * VL + l] - x[(N - 1 - j) * VL + l];
+        }
+    fdct_pow2_v(e, h, E);
+    const float *c = odd_table(N);
+    for (int m = 0; m < h; ++m) {
+        alignas(32) float acc[VL];
+        const float c0 = c[(size_t)m * h];
+        for (int l = 0; l < VL; ++l) {
+            X[2 * m * VL + l] = E[m * VL + l];
+            acc[l] = o[l] * c0;
+        }
+        for (int j = 1; j < h; ++j) {
+            const float cj = c[(size_t)m * h + j];
+            for (int l = 0; l < VL; ++l) acc[l] = std::fmaf(o[j * VL + l], cj, acc[l]);
+        }
+        for (int l = 0; l < VL; ++l) X[(2 * m + 1) * VL + l] = acc[l];
+    }
+}
+
+static void idct_pow2_v(const float *X, int N, float *y)
+{
+    if (N == 1) {
+        for (int l = 0; l < VL; ++l) y[l] = X[l];
+        return;
+    }
+    const int h = N / 2;
+    alignas(32) float ev[128 * VL], E[128 * VL];
+    for (int m = 0; m < h; ++m)
+        for (int l = 0; l < VL; ++l) ev[m * VL + l] = X[2 * m * VL + l];
+    idct_pow2_v(ev, h, E);
+    const float *c = odd_table(N);
+    for (int k = 0; k < h; ++k) {
+        alignas(32) float acc[VL];
+        const float c0 = c[(size_t)k * h];
+        for (int l = 0; l < VL; ++l) acc[l] = X[VL + l] * c0;
+        for (int m = 1; m < h; ++m) {
+            const float cm = c[(size_t)k * h + m];
+            for (int l = 0; l < VL; ++l) acc[l] = std::fmaf(X[(2 * m + 1) * VL + l], cm, acc[l]);
+        }
+        for (int l = 0; l < VL; ++l) {
+            y[k * VL + l] = E[k * VL + l] + acc[l];
+            y[(N - 1 - k) * VL + l] = E[k * VL + l] - acc[l];
+        }
+    }
+}
+
+static void fdct_direct_v(const float *x, int N, float *X)
+{
+    const float *t = direct_table(N, false);
+    for (int k = 0; k < N; ++k) {
+        alignas(32) float acc[VL];
+        const float t0 = t[(size_t)k * N];
+        for (int l = 0; l < VL; ++l) acc[l] = x[l] * t0;
+        for (int j = 1; j < N; ++j) {
+            const float tj = t[(size_t)k * N + j];
+            for (int l = 0; l < VL; ++l) acc[l] = std::fmaf(x[j * VL + l], tj, acc[l]);
+        }
+        for (int l = 0; l < VL; ++l) X[k * VL + l] = acc[l];
+    }
+}
+
+static void idct_direct_v(const float *X, int N, float *y)
+{
+    const float *t = direct_table(N, true);
+    for (int k = 0; k < N; ++k) {
+        alignas(32) float acc[VL];
+        for (int l = 0; l < VL; ++l) acc[l] = X[l];
+        for (int j = 1; j < N; ++j) {
+            const float tj = t[(size_t)k * N + j];
+            for (int l = 0; l < VL; ++l) acc[l] = std::fmaf(X[j * VL + l], tj, acc[l]);
+        }
+        for (int l = 0; l < VL; ++l) y[k * VL + l] = acc[l];
+    }
+}
+
+// Transforms `lanes` (<= VL) strided 1-D sequences of length N: element j of lane l at
+// data[l * lstride + j * jstride].
+static void dct1d_v(float *data, int N, ptrdiff_t jstride, ptrdiff_t lstride, int lanes, bool inverse)
+{
+    alignas(32) float in[256 * VL], out[256 * VL];
+    for (int j = 0; j < N; ++j)
+        for (int l = 0; l < VL; ++l) in[j * VL + l] = l < lanes ? data[l * lstride + j * jstride] : 0.0f;
+    if (is_pow2(N)) { if (inverse) idct_pow2_v(in, N, out); else fdct_pow2_v(in, N, out); }
+    else { if (inverse) idct_direct_v(in, N, out); else fdct_direct_v(in, N, out); }
+    for (int j = 0; j < N; ++j)
+        for (int l = 0; l < lanes; ++l) data[l * lstride + j * jstride] = out[j * VL + l];
+}
+
+static void dct3d(float *g, int n, int B, bool inverse)
+{
+    const ptrdiff_t plane = (ptrdiff_t)B * B;
+    auto rows = [&](bool inv) {        // along x: lanes are rows y
+        for (int z = 0; z < n; ++z)
+            for (int y0 = 0; y0 < B; y0 += VL) dct1d_v(g + z * plane + y0 * B, B, 1, B, std::min(VL, B - y0), inv);
+    };
+    auto cols = [&](bool inv) {        // along y: lanes are columns x
+        for (int z = 0; z < n; ++z)
+            for (int x0 = 0; x0 < B; x0 += VL) dct1d_v(g + z * plane + x0, B, B, 1, std::min(VL, B - x0), inv);
+    };
+    auto zs = [&](bool inv) {          // along z: lanes are coefficient positions
+        for (int p0 = 0; p0 < plane; p0 += VL) dct1d_v(g + p0, n, plane, 1, (int)std::min<ptrdiff_t>(VL, plane - p0), inv);
+    };
+    if (!inverse) { rows(false); cols(false); zs(false); }
+    else { zs(true); cols(true); rows(true); }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1006,6 +1129,7 @@ int oracle_vaggregate(int radius, int nframes_total, int n, int nplanes, const i
 
 // 3-D transform of one group in place (debug/parity of the DCT factorisation).
 void oracle_dct3d(float *g, int n, int B, int inverse) { dct3d(g, n, B, inverse != 0); }
+void oracle_dct3d_scalar(float *g, int n, int B, int inverse) { dct3d_scalar(g, n, B, inverse != 0); }
 
 // Raw tables (debug/parity): odd-part matrix of length N (h*h) and direct tables (N*N).
 void oracle_dct_tables(int N, float *odd, float *fwd, float *inv)

@@ -51,6 +51,7 @@ def lib():
         L.oracle_vbm3d.argtypes = [_P(Params), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F, _F, _F, C.c_int]
         L.oracle_vaggregate.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _I, C.c_int, C.c_int, C.c_int, _F, _F]
         L.oracle_dct3d.argtypes = [_F, C.c_int, C.c_int, C.c_int]
+        L.oracle_dct3d_scalar.argtypes = [_F, C.c_int, C.c_int, C.c_int]
         L.oracle_dct_tables.argtypes = [C.c_int, _F, _F, _F]
         L.oracle_int2float.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F]
         L.oracle_float2int.argtypes = [_F, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
@@ -195,11 +196,12 @@ def vaggregate(radius, stacked, process=(1, 1, 1)):
     return out
 
 
-def dct3d(groups, inverse=False):
+def dct3d(groups, inverse=False, scalar=False):
     g = np.ascontiguousarray(groups, np.float32).copy()
     ng, n, B, _ = g.shape
+    fn = lib().oracle_dct3d_scalar if scalar else lib().oracle_dct3d
     for k in range(ng):
-        lib().oracle_dct3d(fp(g[k]), n, B, int(inverse))
+        fn(fp(g[k]), n, B, int(inverse))
     return g
 
 

@@ -116,6 +116,17 @@ def test_dct_against_definition(orc, n, B):
         assert np.abs(got - exp).max() <= 2e-6 * scale * math.sqrt(n * B * B)
 
 
+@pytest.mark.parametrize("n,B", [(1, 8), (5, 8), (16, 8), (32, 8), (7, 11), (4, 5), (3, 16), (256, 2)])
+def test_vector_dct_equals_scalar_dct(orc, n, B):
+    # the lane-parallel transform performs the scalar operation sequence bit for bit
+    rng = np.random.default_rng(n + 7 * B)
+    g = rng.normal(0, 1, (3, n, B, B)).astype(np.float32)
+    for inverse in (False, True):
+        a = orc.dct3d(g, inverse)
+        b = orc.dct3d(g, inverse, scalar=True)
+        assert np.array_equal(a.view(np.int32), b.view(np.int32))
+
+
 def test_dct_round_trip_amplification(orc):
     # inverse(forward(x)) = 2n * 2B * 2B * x (finalAMP of source/BM3D.cpp:155)
     rng = np.random.default_rng(3)

@@ -37,6 +37,7 @@ def build(force=False, verbose=False):
         return LIB
     os.makedirs(LIB_DIR, exist_ok=True)
     cmd = [nvcc_path(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+           "-I" + os.path.join(os.path.dirname(HERE), "include"),
            "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared", "-cudart", "static",
            "-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
     if verbose:

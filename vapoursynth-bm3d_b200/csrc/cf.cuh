@@ -103,97 +103,271 @@ __device__ __forceinline__ GroupLoc locate(const CFArgs &a, int p, long long grp
     return g;
 }
 
-// ---- fast path: B = 8, full groups of G in {8, 16, 32}; lane = block for the 2-D stages,
-//      lane = coefficient column(s) for the z stage; transposes through padded shared memory ----
+// ---- fast path: B = 8, groups of n <= G blocks, G in {8, 16, 32} ---------------------------------
+// A warp works on 32/G groups at a time.  Lane = block for the 2-D transforms (registers); the
+// transpose buffer T[32][kTP] (row = block, column = 2-D coefficient y*8+x) hands the coefficients
+// to the z stage, where each lane takes 64/G columns.
+
+constexpr int kTP = 65;   // padded row pitch: rows and columns are both bank-conflict free
+
+// z stage of one coefficient column (stride kTP): forward DCT along z, hard threshold with t0
+// (z == 0) / t1 (z > 0) (Basic) or multiplication by the Wiener weights in Wc (Final), inverse
+// DCT along z, in place.  Returns the kept count (Basic) or the column's sum of squared weights
+// (Final).
+template <int G, bool WIENER>
+__device__ __noinline__ float zstage_column(float *Tc, const float *Wc, float t0, float t1)
+{
+    float col[G], X[G];
+#pragma unroll
+    for (int zz = 0; zz < G; ++zz) col[zz] = Tc[zz * kTP];
+    fdct_reg<G>(col, X);
+    float r = 0.0f;
+    if constexpr (!WIENER) {
+        int k = 0;
+#pragma unroll
+        for (int zz = 0; zz < G; ++zz) {
+            const float th = zz == 0 ? t0 : t1;
+            const bool keep = fabsf(X[zz]) > th;
+            k += keep;
+            X[zz] = keep ? X[zz] : 0.0f;
+        }
+        r = (float)k;
+    } else {
+#pragma unroll
+        for (int zz = 0; zz < G; ++zz) {
+            const float w = Wc[zz * kTP];
+            X[zz] = __fmul_rn(X[zz], w);
+            r = __fadd_rn(r, __fmul_rn(w, w));
+        }
+    }
+    idct_reg<G>(X, col);
+#pragma unroll
+    for (int zz = 0; zz < G; ++zz) Tc[zz * kTP] = col[zz];
+    return r;
+}
+
+// Wiener weights of one reference-group column: forward DCT along z, then
+// w = r^2 / (r^2 + sg) written back in place.
+template <int G>
+__device__ __noinline__ void wiener_column(float *Wc, float sg)
+{
+    float col[G], R[G];
+#pragma unroll
+    for (int zz = 0; zz < G; ++zz) col[zz] = Wc[zz * kTP];
+    fdct_reg<G>(col, R);
+#pragma unroll
+    for (int zz = 0; zz < G; ++zz) {
+        const float r2 = __fmul_rn(R[zz], R[zz]);
+        Wc[zz * kTP] = __fdiv_rn(r2, __fadd_rn(r2, sg));
+    }
+}
+
+// Non-power-of-two group length n (< G): direct FMA chains over the n x n tables (the oracle's
+// fdct_direct / idct_direct).
+template <bool WIENER>
+__device__ __noinline__ float zstage_direct(float *Tc, const float *Wc, float t0, float t1, int n, const float *fwd,
+                                            const float *inv)
+{
+    float x[32], X[32];
+    for (int j = 0; j < n; ++j) x[j] = Tc[j * kTP];
+    for (int k = 0; k < n; ++k) {
+        float acc = __fmul_rn(x[0], __ldg(fwd + k * n));
+        for (int j = 1; j < n; ++j) acc = __fmaf_rn(x[j], __ldg(fwd + k * n + j), acc);
+        X[k] = acc;
+    }
+    float r = 0.0f;
+    if constexpr (!WIENER) {
+        int kk = 0;
+        for (int zz = 0; zz < n; ++zz) {
+            const float th = zz == 0 ? t0 : t1;
+            const bool keep = fabsf(X[zz]) > th;
+            kk += keep;
+            X[zz] = keep ? X[zz] : 0.0f;
+        }
+        r = (float)kk;
+    } else {
+        for (int zz = 0; zz < n; ++zz) {
+            const float w = Wc[zz * kTP];
+            X[zz] = __fmul_rn(X[zz], w);
+            r = __fadd_rn(r, __fmul_rn(w, w));
+        }
+    }
+    for (int k = 0; k < n; ++k) {
+        float acc = X[0];
+        for (int j = 1; j < n; ++j) acc = __fmaf_rn(X[j], __ldg(inv + k * n + j), acc);
+        Tc[k * kTP] = acc;
+    }
+    return r;
+}
+
+__device__ __noinline__ void wiener_direct(float *Wc, float sg, int n, const float *fwd)
+{
+    float x[32];
+    for (int j = 0; j < n; ++j) x[j] = Wc[j * kTP];
+    for (int k = 0; k < n; ++k) {
+        float acc = __fmul_rn(x[0], __ldg(fwd + k * n));
+        for (int j = 1; j < n; ++j) acc = __fmaf_rn(x[j], __ldg(fwd + k * n + j), acc);
+        const float r2 = __fmul_rn(acc, acc);
+        Wc[k * kTP] = __fdiv_rn(r2, __fadd_rn(r2, sg));
+    }
+}
+
+template <int G, bool WIENER>
+__device__ __forceinline__ float zstage_any(float *Tc, const float *Wc, float t0, float t1, int n, const float *fwd,
+                                            const float *inv)
+{
+    if (n == G) return zstage_column<G, WIENER>(Tc, Wc, t0, t1);
+    if (G > 16 && n == 16) return zstage_column<(G > 16 ? 16 : 1), WIENER>(Tc, Wc, t0, t1);
+    if (G > 8 && n == 8) return zstage_column<(G > 8 ? 8 : 1), WIENER>(Tc, Wc, t0, t1);
+    if (n == 4) return zstage_column<4, WIENER>(Tc, Wc, t0, t1);
+    if (n == 2) return zstage_column<2, WIENER>(Tc, Wc, t0, t1);
+    if (n == 1) return zstage_column<1, WIENER>(Tc, Wc, t0, t1);
+    return zstage_direct<WIENER>(Tc, Wc, t0, t1, n, fwd, inv);
+}
+
+template <int G>
+__device__ __forceinline__ void wiener_any(float *Wc, float sg, int n, const float *fwd)
+{
+    if (n == G) wiener_column<G>(Wc, sg);
+    else if (G > 16 && n == 16) wiener_column<(G > 16 ? 16 : 1)>(Wc, sg);
+    else if (G > 8 && n == 8) wiener_column<(G > 8 ? 8 : 1)>(Wc, sg);
+    else if (n == 4) wiener_column<4>(Wc, sg);
+    else if (n == 2) wiener_column<2>(Wc, sg);
+    else if (n == 1) wiener_column<1>(Wc, sg);
+    else wiener_direct(Wc, sg, n, fwd);
+}
+
+__device__ __forceinline__ const float *dtab_for(const CFArgs &a, int N, bool inverse)
+{
+    const int off = a.dtab_off[N];
+    return off < 0 ? nullptr : a.dtab + off + (inverse ? N * N : 0);
+}
+
+// The collaborative-filter kernel: per-lane gathers straight into registers, register-resident
+// 2-D transforms, the z stage inline for full groups (out-of-line calls only for the rare partial
+// groups), and per-lane global float atomics into the numerator and per-origin weight planes.
+// Shared memory holds only the transpose buffers (T, and T2 for the Wiener weights).  Measured on
+// B200 against two alternatives -- a shared-memory tile accumulator per CTA and fully out-of-line
+// stages with coalesced gathers -- this layout was the fastest: occupancy and latency hiding
+// matter more here than atomic traffic.
+__device__ __forceinline__ void load_block8(float (&blk)[64], const float *sp, int ld)
+{
+#pragma unroll
+    for (int y = 0; y < 8; ++y)
+#pragma unroll
+        for (int x = 0; x < 8; ++x) blk[y * 8 + x] = __ldg(sp + (long long)y * ld + x);
+}
 
 template <int G, bool WIENER>
 __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
 {
-    constexpr int GPW = 32 / G;      // groups per warp
-    constexpr int C = 64 / G;        // coefficient columns per lane in the z stage
-    constexpr int TP = 65;           // padded row pitch of the transpose buffer
+    constexpr int GPW = 32 / G;
+    constexpr int C = 64 / G;
     extern __shared__ float smem[];
     const int lane = (int)lane_id();
     const int warp = threadIdx.x >> 5;
+    const int nwarp = blockDim.x >> 5;
     const int sub = lane / G;
     const int z = lane - sub * G;
-    float *T = smem + warp * (WIENER ? 2 : 1) * 32 * TP;
-    float *T2 = T + 32 * TP;
+    float *T = smem + warp * (WIENER ? 2 : 1) * 32 * kTP;
+    float *T2 = T + 32 * kTP;
 
-    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long wg = (long long)blockIdx.x * (blockDim.x >> 5) + warp; wg * GPW < a.ngroups; wg += nwarps) {
+    const long long nwarps = (long long)gridDim.x * nwarp;
+    for (long long wg = (long long)blockIdx.x * nwarp + warp; wg * GPW < a.ngroups; wg += nwarps) {
         const long long grp = wg * GPW + sub;
         const bool inrange = grp < a.ngroups;
-        const int n = inrange ? a.count[grp] : 0;
-        const bool active = inrange && n == G;
-        const uint32_t pk = active ? a.pos[grp * G + z] : a.pos[0];
-        const long long g0 = active ? grp : 0;
-
+        const long long g0 = inrange ? grp : 0;
+        const int n = min(a.count[g0], G);
+        const bool active = inrange && z < n;
+        const bool full = __all_sync(0xffffffffu, n == G);
+        const uint32_t pk = a.pos[g0 * G + min(z, n - 1)];
         for (int p = 0; p < 3; ++p) {
             if (!a.process[p]) continue;
             const GroupLoc L = locate(a, p, g0, pk);
             float blk[64];
-            {
-                const float *sp = L.src + (long long)L.y * a.ld + L.x;
-#pragma unroll
-                for (int y = 0; y < 8; ++y)
-#pragma unroll
-                    for (int x = 0; x < 8; ++x) blk[y * 8 + x] = __ldg(sp + (long long)y * a.ld + x);
-            }
-            fwd2d8(blk);
-#pragma unroll
-            for (int e = 0; e < 64; ++e) T[lane * TP + e] = blk[e];
             if constexpr (WIENER) {
-                const float *rp = L.ref + (long long)L.y * a.ld + L.x;
-#pragma unroll
-                for (int y = 0; y < 8; ++y)
-#pragma unroll
-                    for (int x = 0; x < 8; ++x) blk[y * 8 + x] = __ldg(rp + (long long)y * a.ld + x);
+                load_block8(blk, L.ref + (long long)L.y * a.ld + L.x, a.ld);
                 fwd2d8(blk);
 #pragma unroll
-                for (int e = 0; e < 64; ++e) T2[lane * TP + e] = blk[e];
-            }
-            __syncwarp();
-
-            int kept = 0;
-            float l2 = 0.0f;
+                for (int e = 0; e < 64; ++e) T2[lane * kTP + e] = blk[e];
+                __syncwarp();
+                const float sg = a.wsig2[p][n - 1];
+                if (full) {
 #pragma unroll 1
-            for (int q = 0; q < C; ++q) {
-                const int c = z + q * G;             // coefficient column (y*8 + x)
-                float col[G], X[G];
+                    for (int q = 0; q < C; ++q) {
+                        float *Wc = T2 + sub * G * kTP + z + q * G;
+                        float col[G], R[G];
 #pragma unroll
-                for (int zz = 0; zz < G; ++zz) col[zz] = T[(sub * G + zz) * TP + c];
-                fdct_reg<G>(col, X);
-                if constexpr (!WIENER) {
-                    const int fxy = ((c & 7) == 0) + ((c >> 3) == 0);
-                    const float t0 = a.thr4[p][G - 1][fxy + 1];   // z == 0
-                    const float t1 = a.thr4[p][G - 1][fxy];       // z > 0
+                        for (int zz = 0; zz < G; ++zz) col[zz] = Wc[zz * kTP];
+                        fdct_reg<G>(col, R);
 #pragma unroll
-                    for (int zz = 0; zz < G; ++zz) {
-                        const float th = zz == 0 ? t0 : t1;
-                        const bool keep = fabsf(X[zz]) > th;
-                        kept += keep;
-                        X[zz] = keep ? X[zz] : 0.0f;
+                        for (int zz = 0; zz < G; ++zz) {
+                            const float r2 = __fmul_rn(R[zz], R[zz]);
+                            Wc[zz * kTP] = __fdiv_rn(r2, __fadd_rn(r2, sg));
+                        }
                     }
                 } else {
-                    float rc[G], R[G];
-#pragma unroll
-                    for (int zz = 0; zz < G; ++zz) rc[zz] = T2[(sub * G + zz) * TP + c];
-                    fdct_reg<G>(rc, R);
-                    const float sg = a.wsig2[p][G - 1];
-#pragma unroll
-                    for (int zz = 0; zz < G; ++zz) {
-                        const float r2 = __fmul_rn(R[zz], R[zz]);
-                        const float w = __fdiv_rn(r2, __fadd_rn(r2, sg));
-                        X[zz] = __fmul_rn(X[zz], w);
-                        l2 = __fadd_rn(l2, __fmul_rn(w, w));
-                    }
+                    const float *fwd = n == G ? nullptr : dtab_for(a, n, false);
+#pragma unroll 1
+                    for (int q = 0; q < C; ++q) wiener_any<G>(T2 + sub * G * kTP + z + q * G, sg, n, fwd);
                 }
-                idct_reg<G>(X, col);
-#pragma unroll
-                for (int zz = 0; zz < G; ++zz) T[(sub * G + zz) * TP + c] = col[zz];
+                __syncwarp();
             }
-            // reduce over the G lanes of this group
+            load_block8(blk, L.src + (long long)L.y * a.ld + L.x, a.ld);
+            fwd2d8(blk);
+#pragma unroll
+            for (int e = 0; e < 64; ++e) T[lane * kTP + e] = blk[e];
+            __syncwarp();
+            int kept = 0;
+            float l2 = 0.0f;
+            if (full) {
+#pragma unroll 1
+                for (int q = 0; q < C; ++q) {
+                    const int c = z + q * G;
+                    float *Tc = T + sub * G * kTP + c;
+                    float col[G], X[G];
+#pragma unroll
+                    for (int zz = 0; zz < G; ++zz) col[zz] = Tc[zz * kTP];
+                    fdct_reg<G>(col, X);
+                    if constexpr (!WIENER) {
+                        const int fxy = ((c & 7) == 0) + ((c >> 3) == 0);
+                        const float t0 = a.thr4[p][G - 1][fxy + 1];
+                        const float t1 = a.thr4[p][G - 1][fxy];
+#pragma unroll
+                        for (int zz = 0; zz < G; ++zz) {
+                            const float th = zz == 0 ? t0 : t1;
+                            const bool keep = fabsf(X[zz]) > th;
+                            kept += keep;
+                            X[zz] = keep ? X[zz] : 0.0f;
+                        }
+                    } else {
+                        const float *Wc = T2 + sub * G * kTP + c;
+#pragma unroll
+                        for (int zz = 0; zz < G; ++zz) {
+                            const float w = Wc[zz * kTP];
+                            X[zz] = __fmul_rn(X[zz], w);
+                            l2 = __fadd_rn(l2, __fmul_rn(w, w));
+                        }
+                    }
+                    idct_reg<G>(X, col);
+#pragma unroll
+                    for (int zz = 0; zz < G; ++zz) Tc[zz * kTP] = col[zz];
+                }
+            } else {
+                const float *fwd = dtab_for(a, n, false);
+                const float *inv = dtab_for(a, n, true);
+#pragma unroll 1
+                for (int q = 0; q < C; ++q) {
+                    const int c = z + q * G;
+                    const int fxy = ((c & 7) == 0) + ((c >> 3) == 0);
+                    const float t0 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy + 1];
+                    const float t1 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy];
+                    const float r = zstage_any<G, WIENER>(T + sub * G * kTP + c, WIENER ? T2 + sub * G * kTP + c : nullptr,
+                                                          t0, t1, n, n == G ? nullptr : fwd, n == G ? nullptr : inv);
+                    if constexpr (!WIENER) kept += (int)r;
+                    else l2 = __fadd_rn(l2, r);
+                }
+            }
 #pragma unroll
             for (int o = G / 2; o > 0; o >>= 1) {
                 if constexpr (!WIENER) kept += __shfl_xor_sync(0xffffffffu, kept, o);
@@ -201,10 +375,9 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
             }
             __syncwarp();
 #pragma unroll
-            for (int e = 0; e < 64; ++e) blk[e] = T[lane * TP + e];
+            for (int e = 0; e < 64; ++e) blk[e] = T[lane * kTP + e];
             __syncwarp();
             inv2d8(blk);
-
             float denW;
             if constexpr (!WIENER) {
                 denW = kept < 1 ? 1.0f : __fdiv_rn(1.0f, (float)kept);
@@ -212,7 +385,7 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
                 const float eps = 1.1920928955078125e-07f;
                 denW = __fdiv_rn(1.0f, l2 > eps ? l2 : eps);
             }
-            const float numW = __fdiv_rn(denW, a.amp[G - 1]);
+            const float numW = __fdiv_rn(denW, a.amp[n - 1]);
             if (active) {
                 float *np = L.num + (long long)L.y * a.ld + L.x;
 #pragma unroll
@@ -226,12 +399,6 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
 }
 
 // ---- generic path: any B <= 64, any n <= 256; one warp per group, data in global scratch ----
-
-__device__ __forceinline__ const float *dtab_for(const CFArgs &a, int N, bool inverse)
-{
-    const int off = a.dtab_off[N];
-    return off < 0 ? nullptr : a.dtab + off + (inverse ? N * N : 0);
-}
 
 __device__ void dct3d_warp(float *g, int n, int B, bool inverse, const CFArgs &a, float *tmp)
 {

@@ -6,7 +6,7 @@
 // aggregation (K3+K4), normalisation / stacking (K5), conversion back to the output format and,
 // for host frames, device -> host copies.  Everything between the conversions stays on the GPU.
 
-#include "../../include/bm3d_b200.h"
+#include "bm3d_b200.h"
 
 #include <cuda_runtime.h>
 
@@ -1018,14 +1018,17 @@ public:
             const long long grid = std::max<long long>(1, std::min<long long>((warps_needed + warps - 1) / warps, 148LL * 64));
             CU(launch_cf_fast(a, warps, (int)grid, stream));
         }
-        // generic path: groups the fast kernel does not cover (partial groups or other shapes)
-        const long long slot_floats = (long long)para.G * para.B * para.B * 2;
-        long long gwarps = std::min<long long>(148LL * 16, std::max<long long>(1, (1LL << 28) / (slot_floats * 4)));
-        gwarps = std::max<long long>(4, gwarps / 4 * 4);
-        a.scratch = static_cast<float *>(scratch.get(sizeof(float) * slot_floats * gwarps));
-        a.scratch_per_warp = slot_floats;
-        a.skip_full = fast ? 1 : 0;
-        CU(launch_cf_generic(a, 4, (int)(gwarps / 4), stream));
+        if (!fast) {
+            // generic path: block sizes other than 8 and group sizes outside {8, 16, 32}; one warp
+            // per group with a global scratch slot per resident warp (at most 1 GiB in total)
+            const long long slot_floats = (long long)para.G * para.B * para.B * 2;
+            long long gwarps = std::min<long long>(148LL * 16, std::max<long long>(1, (1LL << 28) / (slot_floats * 4)));
+            gwarps = std::max<long long>(4, gwarps / 4 * 4);
+            a.scratch = static_cast<float *>(scratch.get(sizeof(float) * slot_floats * gwarps));
+            a.scratch_per_warp = slot_floats;
+            a.skip_full = 0;
+            CU(launch_cf_generic(a, 4, (int)(gwarps / 4), stream));
+        }
     }
 
     int matches(int k, int *counts, int *zs, int *ys, int *xs, float *keys, int cap) override

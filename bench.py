@@ -184,7 +184,7 @@ def lattice_count(pos, lim, rng):
 
 
 def algorithmic_work(width, height, frames, step, G, n_mean, wiener):
-    """SURVEY-style algorithmic FLOPs of one call: BM = 3*B^2 per evaluated candidate (sub, mul,
+    """Algorithmic FLOPs of one call: BM = 3*B^2 per evaluated candidate (sub, mul,
     add per pixel); DCT = dense separable count 2*(n*2B^3 + B^2*n^2) per transform, 2 transforms
     (Basic) or 3 (Final) per group and plane, 3 planes."""
     B, R = 8, 16
@@ -245,7 +245,7 @@ def ours_arm(args):
     import numpy as np
     import torch
     from bm3d_b200 import _capi as capi
-    from bm3d_b200 import synth
+    from bm3d_b200 import shard, synth
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -258,8 +258,9 @@ def ours_arm(args):
 
     L = capi.lib()
     F, Wd, Hd = args.frames, args.width, args.height
-    # synthetic frames: each rank its own seeds (frame sharding)
-    nz, clean = synth.rgb_frames(1 + rank, F, Hd, Wd, SIGMA)
+    # frame sharding: the clip has F frames per rank; this rank filters its contiguous range
+    first, count = shard.frame_range(F * world, rank, world)
+    nz, clean = synth.rgb_frames(1, count, Hd, Wd, SIGMA, first=first)
     rgb_in = torch.from_numpy(nz).cuda()
     stream = torch.cuda.Stream()
     vi = capi.VideoInfo(capi.RGB, capi.FLOAT, 32, 0, 0, Wd, Hd, F)
@@ -408,7 +409,7 @@ def ours_arm(args):
                          "peak": round(peak, 3) if peak else None, "unit": "TFLOP/s",
                          "frac": round(achieved / peak, 4) if (achieved and peak) else None, "traffic": traffic,
                          "peak_source": "measured in-process: cuBLAS SGEMM FP32 (TF32 off), 8192^3 best of 5",
-                         "work": "SURVEY 8(d) algorithmic FLOPs: BM 3*B^2 per candidate; DCT 2*(n*2B^3+B^2*n^2) per transform"},
+                         "work": "algorithmic FLOPs: block matching 3*B^2 per evaluated candidate; transforms 2*(n*2B^3+B^2*n^2) per 3-D DCT of a group of n blocks (2 per group and plane for Basic, 3 for Final)"},
             "stages_ms": {"basic": [round(v, 3) for v in stage["basic"]], "final": [round(v, 3) for v in stage["final"]],
                           "order": ["ingest", "block_matching", "predictive", "collaborative_filter", "normalise", "egress"]},
             "e2e": {"value": round(v_e2e, 3), "unit": "Mpix/s", "h2d_bytes_per_step": int(nz.nbytes),

@@ -90,18 +90,22 @@ def to_u16(x):
     return np.clip(np.round(65535.0 * x), 0, 65535).astype(np.uint16)
 
 
-def gray_frames(config, nframes, h, w, sigma):
-    """[nframes][1][h][w] float32 noisy frames and their clean counterparts."""
-    clean = np.stack([clean_gray(h, w, config * 1000 + f * 10)[None] for f in range(nframes)])
-    nz = np.stack([noisy(clean[f], sigma, config * 1000 + f * 10 + 5) for f in range(nframes)])
+def gray_frames(config, nframes, h, w, sigma, first=0):
+    """[nframes][1][h][w] float32 noisy frames first..first+nframes-1 of a clip, and their clean
+    counterparts."""
+    fr = range(first, first + nframes)
+    clean = np.stack([clean_gray(h, w, config * 1000 + f * 10)[None] for f in fr])
+    nz = np.stack([noisy(clean[i], sigma, config * 1000 + f * 10 + 5) for i, f in enumerate(fr)])
     return nz.astype(np.float32), clean.astype(np.float32)
 
 
-def rgb_frames(config, nframes, h, w, sigma):
-    """[nframes][3][h][w] float32 noisy RGB frames (correlated channels) and clean frames."""
-    clean = np.stack([clean_rgb(h, w, config * 1000 + f * 10) for f in range(nframes)])
-    nz = np.stack([np.stack([noisy(clean[f, c], sigma, config * 1000 + f * 10 + c) for c in range(3)])
-                   for f in range(nframes)])
+def rgb_frames(config, nframes, h, w, sigma, first=0):
+    """[nframes][3][h][w] float32 noisy RGB frames first..first+nframes-1 of a clip (correlated
+    channels), and their clean counterparts."""
+    fr = range(first, first + nframes)
+    clean = np.stack([clean_rgb(h, w, config * 1000 + f * 10) for f in fr])
+    nz = np.stack([np.stack([noisy(clean[i, c], sigma, config * 1000 + f * 10 + c) for c in range(3)])
+                   for i, f in enumerate(fr)])
     return nz.astype(np.float32), clean.astype(np.float32)
 
 

@@ -135,6 +135,31 @@ BM3D_API const char *bm3d_get_error(void);
 typedef void (*bm3d_log_fn)(int level, const char *message, void *user);
 BM3D_API void bm3d_set_log_callback(bm3d_log_fn fn, void *user);
 
+/* ---- allocation-free Basic estimate of one plane ----------------------------------------------
+ * No counterpart in the reference (the plugin allocates its buffers per frame).  For callers that
+ * cannot let a library call cudaMalloc: hosts that give all of the GPU's memory to their own pool
+ * allocator at start-up, where an outside allocation fails or breaks their accounting, and
+ * real-time pipelines that forbid cudaMalloc / cudaFree because those calls synchronise the whole
+ * device.  The filter objects above allocate workspaces on first use; this call allocates nothing.
+ *
+ * Computes bm3d.Basic(clip, profile=profile, sigma=sigma) for one 32-bit float GRAY plane, every
+ * other argument at its default.  src and dst are device pointers with `stride` bytes between
+ * rows (a multiple of 4, at least width * 4); profile NULL means "fast".  Work is queued on
+ * `stream` (a cudaStream_t; NULL is the legacy default stream) and the call returns without
+ * waiting for it.
+ *
+ * Its work buffers are one fixed 48 MiB device array inside the library, held by every GPU that
+ * loads the library's device code until the process exits.  A plane that needs more (1920x1080
+ * fits at every profile; a 3840x2160 plane does not) is rejected with BM3D_ERR_UNSUPPORTED and a
+ * message that gives the size it needed.  The first call on a device sets that device up (finds the
+ * array's device address and copies constant tables with synchronous copies): make that first call
+ * before any stream capture on the device.  All calls share the one array, which keeps the last
+ * call's contents; each call clears what must start at zero, but calls that overlap on the GPU
+ * (different streams, or host threads that do not order their calls) race and corrupt each
+ * other's results, so order them on one stream. */
+BM3D_API int bm3d_basic_noalloc(const float *src, float *dst, int width, int height, int64_t stride,
+                                const char *profile, double sigma, void *cuda_stream);
+
 /* ---- inspection entry points (tests and tooling) ---------------------------------------------
  * Match lists of the last bm3d_get_frames call of a Basic/Final/VBasic/VFinal filter, for output
  * frame k of that batch, in reference-block scan order (row-major over the clamped scan of

@@ -1,7 +1,7 @@
 """Build recipe for the in-tree shared library lib/libbm3d_b200.so (sm_100a).
 
-Compiles csrc/kernels.cu (every kernel) and csrc/host.cpp (argument processing, filter objects,
-C ABI of include/bm3d_b200.h) with nvcc, linking the CUDA runtime statically so the library only
+Compiles csrc/kernels.cu (every kernel), csrc/host.cpp (argument processing, filter objects,
+C ABI of include/bm3d_b200.h) and csrc/noalloc.cu (the allocation-free Basic entry point) with nvcc, linking the CUDA runtime statically so the library only
 needs the NVIDIA driver at run time.
 """
 import os
@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libbm3d_b200.so")
-SOURCES = ["kernels.cu", "host.cpp"]
+SOURCES = ["kernels.cu", "host.cpp", "noalloc.cu"]
 DEPS = SOURCES + ["args.h", "bm.cuh", "cf.cuh", "common.cuh", "convert.cuh", "launch.h", "params.h",
                   "select.cuh", "vbm.cuh", os.path.join("..", "..", "include", "bm3d_b200.h")]
 

@@ -40,6 +40,10 @@ static int fail(int code, const std::string &msg)
     return code;
 }
 
+// Error text for the entry points defined in other translation units.
+int set_error(int code, const std::string &msg) { return fail(code, msg); }
+void clear_error() { g_error.clear(); }
+
 static void log_warning(const std::string &msg)
 {
     std::lock_guard<std::mutex> lk(g_log_mutex);

@@ -14,7 +14,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libbm3d_b200.so")
 SOURCES = ["kernels.cu", "host.cpp", "noalloc.cu"]
-DEPS = SOURCES + ["args.h", "bm.cuh", "cf.cuh", "common.cuh", "convert.cuh", "launch.h", "params.h",
+DEPS = SOURCES + ["args.h", "bm.cuh", "cf.cuh", "cf_tc.cuh", "tc.cuh", "common.cuh", "convert.cuh", "launch.h", "params.h",
                   "select.cuh", "vbm.cuh", os.path.join("..", "..", "include", "bm3d_b200.h")]
 
 

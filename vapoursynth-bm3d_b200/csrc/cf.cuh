@@ -278,7 +278,10 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
         const bool inrange = grp < a.ngroups;
         const long long g0 = inrange ? grp : 0;
         const int n = min(a.count[g0], G);
-        const bool active = inrange && z < n;
+        // skip_full: full groups were filtered by the tensor-core kernel; only partial ones here
+        const bool taken = a.skip_full && n == G;
+        if (__all_sync(0xffffffffu, taken || !inrange)) continue;
+        const bool active = inrange && z < n && !taken;
         const bool full = __all_sync(0xffffffffu, n == G);
         const uint32_t pk = a.pos[g0 * G + min(z, n - 1)];
         for (int p = 0; p < 3; ++p) {

@@ -1,0 +1,318 @@
+// cf_tc.cuh -- precision form of the collaborative filter: the 3-D DCTs of full groups as tf32
+// matrix products on the sm_100a tensor cores (tcgen05, fp32 accumulation in tensor memory).
+//
+// Same arithmetic contract as cf_fast_kernel (source/BM3D_Basic.cpp:72-148,
+// source/BM3D_Final.cpp:50-127, aggregation include/Block.h:1239-1387) except that the transforms
+// are dense matrix products with tf32 operands, so coefficients carry ~2^-11 relative error: the
+// output is close to, not bit-identical with, the plain FP32 path.  Only full groups (n == G) are
+// handled here; the plain kernel filters the partial ones in the same pass over the match lists.
+//
+// A tile is 128 blocks = 128 / G groups of one plane, handled by one warpgroup (128 threads);
+// thread r owns row r = block (r % G) of group r / G.  A CTA runs several warpgroups, each on its
+// own stream of tiles with its own shared-memory operands, mbarrier and 128 tensor-memory columns,
+// so that one warpgroup's gathers and atomics overlap another's tensor-core work; the DCT tables
+// are shared.  Every shared-memory operand is K-major (the tf32 kind takes no MN-major operands):
+//   1. gather  X[b][pixel] (A operand, 128-byte swizzle); Final also gathers the reference group
+//      R.  A warp loads one block per step (lane = pixel row / column), so each load touches the
+//      block's own 4 rows instead of 32 blocks; the block origins come from the owning lanes by
+//      shuffles
+//   2. 2-D DCT Y = X . K2 into tensor memory cols [0, 64) (ref [64, 128))
+//   3. transpose: each thread reads its row of Y and writes it as column b of Yt[coef][b], a B
+//      operand with 128-byte swizzle (conflict-free column writes); Final stacks the reference
+//      coefficients below (rows 64..127), so one N = 128 product transforms both
+//   4. z-DCT   Z = Zf_w . Yt_w per group w into cols [0, 64) (ref [64, 128)); the A operand
+//      Zf_w is a 128-row window of a zero-padded stack around one copy of the G x G DCT matrix,
+//      so that group w lands in rows [G w, G w + G)
+//   5. shrink  thread r owns row (group, z-frequency) of 64 coefficients: hard threshold (Basic)
+//      or Wiener weights from the reference spectrum (Final); the group's count / L2 is a
+//      reduction over its G lanes; S goes back to shared memory as St[coef][kz] (swizzled B)
+//   6. inverse z into cols [0, 64), then inverse 2-D with A read from tensor memory into
+//      cols [64, 128)
+//   7. aggregate: the inverse rows go through shared memory so that a warp adds one block per
+//      step with lane = pixel (one 32-byte sector per block row and atomic instruction instead of
+//      32 scattered sectors); the block weight goes to the weight map as in the plain kernel.
+// Every wait on the tensor cores is bounded; on time-out the warpgroup records the failure in
+// *status and stops; the CTA releases its tensor memory and returns.
+#pragma once
+
+#include "args.h"
+#include "cf.cuh"
+#include "tc.cuh"
+
+namespace bm3d {
+
+// Byte layout of the constant tables in shared memory (host builds the same image).
+template <int G>
+struct TcLayout {
+    static constexpr int kGroups = 128 / G;            // groups per tile
+    static constexpr int kZRows = 256 - G;             // zero-padded stack of the G x G DCT matrix
+    static constexpr int kZBytes = kZRows * G * 4;
+    static constexpr int kKBytes = 64 * 64 * 4;
+    static constexpr int kZf = 0;                       // forward z matrix stack (K-major)
+    static constexpr int kZi = kZf + kZBytes;           // inverse z matrix stack (K-major)
+    static constexpr int kKf = kZi + kZBytes;           // forward 2-D matrix, [coef][pixel] (K-major)
+    static constexpr int kKi = kKf + kKBytes;           // inverse 2-D matrix, [pixel][coef] (K-major)
+    static constexpr int kTableBytes = kKi + kKBytes;
+    static constexpr int kXBytes = 128 * 64 * 4;        // one 128 x 64 data operand
+};
+
+// warpgroups per CTA: shared memory holds the tables and, per warpgroup, one (Basic) or two
+// (Final) 32 KB operands; tensor memory gives 128 columns to each of at most 4
+template <int G, bool WIENER>
+struct TcShape {
+    static constexpr int kWG = WIENER ? 2 : 4;
+    static constexpr int kData = TcLayout<G>::kXBytes * (WIENER ? 2 : 1);
+    static constexpr int kSmem = kData * kWG + TcLayout<G>::kTableBytes;
+};
+
+// byte offset of element (row, k) of a K-major operand with `kdim` columns
+__host__ __device__ constexpr uint32_t tc_kmajor(int row, int k, int kdim)
+{
+    return (uint32_t)((row / 8) * (kdim / 4) * 128 + (k / 4) * 128 + (row % 8) * 16 + (k % 4) * 4);
+}
+
+constexpr uint32_t kTcWaitLimit = 1u << 24;
+
+template <int G, bool WIENER>
+__global__ void __launch_bounds__(128 * TcShape<G, WIENER>::kWG, 1)
+cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
+{
+    using Lay = TcLayout<G>;
+    using Shp = TcShape<G, WIENER>;
+    constexpr int GPT = Lay::kGroups;
+    constexpr int NWG = Shp::kWG;
+    constexpr int NT = WIENER ? 128 : 64;            // rows of the z-stage B operand
+    extern __shared__ __align__(1024) unsigned char tsm[];
+    __shared__ __align__(8) uint64_t mbar[NWG];
+    __shared__ uint32_t tslot;
+
+    const int wg = threadIdx.x >> 7;
+    const int r = threadIdx.x & 127;                 // row of the tile
+    const int warp = threadIdx.x >> 5;
+    const uint32_t bar_id = 1 + wg;
+    const int wsub = r / G;                          // group within the tile
+    const int j = r % G;                             // block index in the group / z-frequency
+    unsigned char *D = tsm + Shp::kData * wg;        // X | R, then Yt, then St
+    unsigned char *tab = tsm + Shp::kData * NWG;
+
+    for (int i = threadIdx.x; i < Lay::kTableBytes / 16; i += blockDim.x)
+        reinterpret_cast<float4 *>(tab)[i] = tables[i];
+    if (warp == 0) tc::tmem_alloc(&tslot, 128 * NWG);
+    if (r == 0) tc::mbar_init(&mbar[wg], 1);
+    tc::fence_proxy_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tm = tslot;
+    const uint32_t tb = tm + 128 * wg;               // this warpgroup's columns
+    const uint32_t lrow = (uint32_t)(32 * (warp & 3)) << 16;
+    const uint32_t sZf = tc::smem_u32(tab + Lay::kZf), sZi = tc::smem_u32(tab + Lay::kZi);
+    const uint32_t sKf = tc::smem_u32(tab + Lay::kKf), sKi = tc::smem_u32(tab + Lay::kKi);
+    const uint32_t sD = tc::smem_u32(D);
+    constexpr uint32_t ID64 = tc::idesc_tf32(128, 64, 0, 0);
+    constexpr uint32_t IDZ = tc::idesc_tf32(128, NT, 0, 0);
+    uint64_t *mb = &mbar[wg];
+    uint32_t phase = 0;
+
+    auto wait_mma = [&]() -> bool {
+        const bool ok = tc::mbar_wait_bounded(mb, phase, kTcWaitLimit);
+        phase ^= 1u;
+        tc::fence_after_sync();
+        return tc::wg_and(bar_id, ok);
+    };
+    auto publish = [&]() {
+        tc::fence_proxy_async_smem();
+        tc::fence_before_sync();
+        tc::wg_sync(bar_id);
+        tc::fence_after_sync();
+    };
+    // 2-D stage, A in shared memory: D[d0, +64) = X . K (X swizzled [128][64], K [64 n][64 k])
+    auto xy_ss = [&](uint32_t d0, uint32_t sx, uint32_t sk) {
+#pragma unroll 1
+        for (int s = 0; s < 8; ++s)
+            tc::mma_ss_tf32(tb + d0, tc::make_desc_sw128(sx + (s / 4) * 16 * 1024 + (s % 4) * 32, 1024),
+                            tc::make_desc(sk + s * 256, 128, 2048), ID64, s > 0);
+    };
+    // 2-D stage, A in tensor memory: D[d0, +64) = T[a0, +64) . K
+    auto xy_ts = [&](uint32_t d0, uint32_t a0, uint32_t sk) {
+#pragma unroll 1
+        for (int s = 0; s < 8; ++s)
+            tc::mma_ts_tf32(tb + d0, tb + a0 + 8 * s, tc::make_desc(sk + s * 256, 128, 2048), ID64, s > 0);
+    };
+    // z stage: D[d0, +nt) = sum_w Zwin_w . Bt_w, Bt swizzled [nt rows][128 k], K range of group w
+    auto z_stage = [&](uint32_t d0, uint32_t sz, int nt, uint32_t idesc) {
+#pragma unroll 1
+        for (int w = 0; w < GPT; ++w)
+#pragma unroll 1
+            for (int s = 0; s < G / 8; ++s) {
+                const uint32_t arow = (uint32_t)((128 - G) - G * w);
+                const uint64_t ad = tc::make_desc(sz + (arow / 8) * (G / 4) * 128 + s * 256, 128, (G / 4) * 128);
+                const uint32_t k0 = (uint32_t)(G * w + 8 * s);
+                const uint64_t bd = tc::make_desc_sw128(sD + (k0 / 32) * (nt / 8) * 1024 + ((k0 % 32) / 8) * 32, 1024);
+                tc::mma_ss_tf32(tb + d0, ad, bd, idesc, !(w == 0 && s == 0));
+            }
+    };
+    // this thread's row of tensor memory (cols c0..c0+63) -> column r, rows row0.., of Bt
+    auto row_to_column = [&](uint32_t c0, int row0, int nt) {
+        float v[64];
+#pragma unroll
+        for (int q = 0; q < 64; q += 16) tc::tmem_ld16(tb + lrow + c0 + q, *reinterpret_cast<float (*)[16]>(v + q));
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int e = 0; e < 64; ++e) *reinterpret_cast<float *>(D + tc::sw128_offset(row0 + e, r, nt)) = v[e];
+    };
+
+    bool failed = false;
+    for (long long tile = (long long)blockIdx.x * NWG + wg; tile < ntiles && !failed; tile += (long long)gridDim.x * NWG) {
+        const long long grp = tile * GPT + wsub;
+        const bool inrange = grp < a.ngroups;
+        const long long g0 = inrange ? grp : 0;
+        const int n = a.count[g0];
+        const bool mine = inrange && n >= G;          // full group: filtered here
+        const uint32_t pk = a.pos[g0 * G + j];
+        for (int p = 0; p < 3 && !failed; ++p) {
+            if (!a.process[p]) continue;
+            const GroupLoc L = locate(a, p, g0, pk);
+            // 1. gather (rows of foreign or partial groups are zero), one block per warp step
+            {
+                const float *sp = L.src + (long long)L.y * a.ld + L.x;
+                const float *rp = L.ref + (long long)L.y * a.ld + L.x;
+                const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
+                const int b0 = r & ~31;
+#pragma unroll 4
+                for (int i = 0; i < 32; ++i) {
+                    const bool mi = __shfl_sync(0xffffffffu, mine, i);
+                    const float *si = reinterpret_cast<const float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(sp), i));
+                    float v0 = 0.f, v1 = 0.f;
+                    if (mi) {
+                        v0 = __ldg(si + (long long)ry * a.ld + cx);
+                        v1 = __ldg(si + (long long)(ry + 4) * a.ld + cx);
+                    }
+                    *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128)) = v0;
+                    *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
+                    if constexpr (WIENER) {
+                        const float *ri = reinterpret_cast<const float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(rp), i));
+                        float u0 = 0.f, u1 = 0.f;
+                        if (mi) {
+                            u0 = __ldg(ri + (long long)ry * a.ld + cx);
+                            u1 = __ldg(ri + (long long)(ry + 4) * a.ld + cx);
+                        }
+                        *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128)) = u0;
+                        *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane + 32, 128)) = u1;
+                    }
+                }
+            }
+            publish();
+            // 2. 2-D DCT
+            if (r == 0) {
+                xy_ss(0, sD, sKf);
+                if constexpr (WIENER) xy_ss(64, sD + Lay::kXBytes, sKf);
+                tc::mma_commit(mb);
+            }
+            if (!wait_mma()) { failed = true; break; }
+            // 3. transpose into the z-stage B operand (reference rows below the source rows)
+            row_to_column(0, 0, NT);
+            if constexpr (WIENER) row_to_column(64, 64, NT);
+            publish();
+            // 4. z-DCT of source (and reference) in one pass
+            if (r == 0) {
+                z_stage(0, sZf, NT, IDZ);
+                tc::mma_commit(mb);
+            }
+            if (!wait_mma()) { failed = true; break; }
+            // 5. shrinkage, one row of 64 coefficients per thread
+            float acc = 0.0f;
+#pragma unroll
+            for (int c0 = 0; c0 < 64; c0 += 32) {
+                float z[32];
+                tc::tmem_ld16(tb + lrow + c0, *reinterpret_cast<float (*)[16]>(z));
+                tc::tmem_ld16(tb + lrow + c0 + 16, *reinterpret_cast<float (*)[16]>(z + 16));
+                if constexpr (WIENER) {
+                    float rr[32];
+                    tc::tmem_ld16(tb + lrow + 64 + c0, *reinterpret_cast<float (*)[16]>(rr));
+                    tc::tmem_ld16(tb + lrow + 64 + c0 + 16, *reinterpret_cast<float (*)[16]>(rr + 16));
+                    tc::tmem_wait_ld();
+                    const float sg = a.wsig2[p][G - 1];
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) {
+                        const float r2 = rr[e] * rr[e];
+                        const float w = __fdividef(r2, r2 + sg);
+                        z[e] *= w;
+                        acc = fmaf(w, w, acc);
+                    }
+                } else {
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) {
+                        const int c = c0 + e;
+                        const int flag = (j == 0) + ((c & 7) == 0) + ((c >> 3) == 0);
+                        const bool keep = fabsf(z[e]) > a.thr4[p][G - 1][flag];
+                        acc += keep ? 1.0f : 0.0f;
+                        z[e] = keep ? z[e] : 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < 32; ++e) *reinterpret_cast<float *>(D + tc::sw128_offset(c0 + e, r, 64)) = z[e];
+            }
+#pragma unroll
+            for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            float denW;
+            if constexpr (WIENER) {
+                const float eps = 1.1920928955078125e-07f;
+                denW = 1.0f / (acc > eps ? acc : eps);
+            } else {
+                denW = acc < 1.0f ? 1.0f : 1.0f / acc;
+            }
+            const float numW = denW / a.amp[G - 1];
+            publish();
+            // 6. inverse z, then inverse 2-D
+            if (r == 0) {
+                z_stage(0, sZi, 64, ID64);
+                tc::mma_commit(mb);
+            }
+            if (!wait_mma()) { failed = true; break; }
+            if (r == 0) {
+                xy_ts(64, 0, sKi);
+                tc::mma_commit(mb);
+            }
+            if (!wait_mma()) { failed = true; break; }
+            // 7. aggregation: rows -> shared memory (this warp's 32 rows), then one block per step
+            {
+                float v[64];
+#pragma unroll
+                for (int c0 = 0; c0 < 64; c0 += 16) tc::tmem_ld16(tb + lrow + 64 + c0, *reinterpret_cast<float (*)[16]>(v + c0));
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 64; c += 4)
+                    *reinterpret_cast<float4 *>(D + tc::sw128_offset(r, c, 128)) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+                __syncwarp();
+                float *np = L.num + (long long)L.y * a.ld + L.x;
+                const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
+                const int b0 = r & ~31;
+#pragma unroll 4
+                for (int i = 0; i < 32; ++i) {
+                    const bool mi = __shfl_sync(0xffffffffu, mine, i);
+                    float *ni = reinterpret_cast<float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(np), i));
+                    const float wi = __shfl_sync(0xffffffffu, numW, i);
+                    if (mi) {
+                        const float x0 = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane, 128));
+                        const float x1 = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128));
+                        atomicAdd(ni + (long long)ry * a.ld + cx, x0 * wi);
+                        atomicAdd(ni + (long long)(ry + 4) * a.ld + cx, x1 * wi);
+                    }
+                }
+            }
+            if (mine) atomicAdd(L.wmap + (long long)L.y * a.ld + L.x, denW);
+            tc::fence_before_sync();
+            tc::wg_sync(bar_id);
+            tc::fence_after_sync();
+        }
+    }
+    if (failed && r == 0) atomicExch(status, 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (warp == 0) tc::tmem_free(tm, 128 * NWG);
+}
+
+}  // namespace bm3d

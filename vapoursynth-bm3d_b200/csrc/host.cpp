@@ -158,25 +158,25 @@ static const std::vector<ArgSpec> &argspec(const std::string &fn)
         {"input", 3, false, false}, {"ref", 3, false, true}, {"profile", 2, false, true},
         {"sigma", 1, true, true}, {"block_size", 0, false, true}, {"block_step", 0, false, true},
         {"group_size", 0, false, true}, {"bm_range", 0, false, true}, {"bm_step", 0, false, true},
-        {"th_mse", 1, false, true}, {"hard_thr", 1, false, true}, {"matrix", 0, false, true}};
+        {"th_mse", 1, false, true}, {"hard_thr", 1, false, true}, {"matrix", 0, false, true}, {"precision", 2, false, true}};
     static const std::vector<ArgSpec> fin = {
         {"input", 3, false, false}, {"ref", 3, false, false}, {"profile", 2, false, true},
         {"sigma", 1, true, true}, {"block_size", 0, false, true}, {"block_step", 0, false, true},
         {"group_size", 0, false, true}, {"bm_range", 0, false, true}, {"bm_step", 0, false, true},
-        {"th_mse", 1, false, true}, {"matrix", 0, false, true}};
+        {"th_mse", 1, false, true}, {"matrix", 0, false, true}, {"precision", 2, false, true}};
     static const std::vector<ArgSpec> vbasic = {
         {"input", 3, false, false}, {"ref", 3, false, true}, {"profile", 2, false, true},
         {"sigma", 1, true, true}, {"radius", 0, false, true}, {"block_size", 0, false, true},
         {"block_step", 0, false, true}, {"group_size", 0, false, true}, {"bm_range", 0, false, true},
         {"bm_step", 0, false, true}, {"ps_num", 0, false, true}, {"ps_range", 0, false, true},
         {"ps_step", 0, false, true}, {"th_mse", 1, false, true}, {"hard_thr", 1, false, true},
-        {"matrix", 0, false, true}};
+        {"matrix", 0, false, true}, {"precision", 2, false, true}};
     static const std::vector<ArgSpec> vfinal = {
         {"input", 3, false, false}, {"ref", 3, false, false}, {"profile", 2, false, true},
         {"sigma", 1, true, true}, {"radius", 0, false, true}, {"block_size", 0, false, true},
         {"block_step", 0, false, true}, {"group_size", 0, false, true}, {"bm_range", 0, false, true},
         {"bm_step", 0, false, true}, {"ps_num", 0, false, true}, {"ps_range", 0, false, true},
-        {"ps_step", 0, false, true}, {"th_mse", 1, false, true}, {"matrix", 0, false, true}};
+        {"ps_step", 0, false, true}, {"th_mse", 1, false, true}, {"matrix", 0, false, true}, {"precision", 2, false, true}};
     static const std::vector<ArgSpec> vagg = {
         {"input", 3, false, false}, {"radius", 0, false, true}, {"sample", 0, false, true}};
     static const std::vector<ArgSpec> none;
@@ -578,6 +578,8 @@ public:
     virtual int run(int n, int count, const bm3d_frame *const *src, const bm3d_frame *const *ref,
                     bm3d_frame *const *dst, bool sync) = 0;
     virtual int matches(int, int *, int *, int *, int *, float *, int) { return -1; }
+    // called after the filter's stream was synchronised (device-side error flags)
+    virtual void synced() {}
     int nplanes() const { return vi.color_family == BM3D_GRAY ? 1 : 3; }
     void init_stream()
     {
@@ -692,6 +694,7 @@ class BM3DBase : public Filter {
 public:
     bool wiener = false;
     bool vbm3d = false;
+    bool tc = false;            // precision form: tensor-core transforms (argument "precision")
     Params para, para_default;
     int matrix = MAT_UNSPEC;
     int process[3] = {1, 1, 1};
@@ -817,6 +820,14 @@ public:
             else if (para.lambda <= 0)
                 return fail(BM3D_ERR_ARG, err("Invalid \"hard_thr\" assigned, must be a positive floating point number"));
         }
+        // extension: "precision" selects the plain FP32 transforms ("fp32", default) or the
+        // tensor-core precision form ("tf32")
+        const char *prec = map_get_data(in, "precision", 0, &error);
+        if (!error) {
+            const std::string pr(prec);
+            if (pr == "tf32") tc = true;
+            else if (pr != "fp32") return fail(BM3D_ERR_ARG, err("Invalid \"precision\" assigned, must be \"fp32\" or \"tf32\""));
+        }
         return BM3D_OK;
     }
 
@@ -847,6 +858,7 @@ public:
     DevBuf m_pos, m_n, m_key, v_pos, v_n, v_key;
     DevBuf d_sy, d_sx, scratch;
     DevBuf d_winb, d_winl, d_winc, d_slot0;
+    DevBuf tc_tab, tc_status;
     DirectTables dtabs;
     int last_count = 0;
 
@@ -864,7 +876,24 @@ public:
         for (int n = 1; n <= para.G; ++n) lengths.push_back(n);
         lengths.push_back(para.B);
         build_direct_tables(dtabs, lengths);
+        if (tc && cf_tc_supported(para.B, para.G)) {
+            std::vector<unsigned char> img;
+            cf_tc_tables(para.G, img);
+            CU(cudaMemcpy(tc_tab.get(img.size()), img.data(), img.size(), cudaMemcpyHostToDevice));
+            CU(cudaMemset(tc_status.get(sizeof(int)), 0, sizeof(int)));
+        }
         return BM3D_OK;
+    }
+
+    void synced() override { check_tc_status(); }
+
+    // time-out flag of the tensor-core kernel (read after the stream is synchronised)
+    void check_tc_status()
+    {
+        if (!tc_status.p) return;
+        int st = 0;
+        CU(cudaMemcpy(&st, tc_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (st) throw std::runtime_error(err("tensor-core collaborative filter timed out"));
     }
 
     // float workspace conversion of one input frame set into plane slot `slot`
@@ -1015,6 +1044,11 @@ public:
         a.dtab = dtabs.tab.as<float>();
         a.dtab_off = dtabs.off.as<int>();
         const bool fast = cf_fast_supported(para.B, para.G);
+        if (fast && tc && tc_tab.p) {
+            // precision form: full groups on the tensor cores, partial ones on the plain kernel
+            CU(launch_cf_tc(a, tc_tab.p, tc_status.as<int>(), stream));
+            a.skip_full = 1;
+        }
         if (fast) {
             const int GPW = 32 / para.G;
             const long long warps_needed = (ngroups + GPW - 1) / GPW;
@@ -1192,6 +1226,7 @@ public:
         if (sync) {
             CU(cudaStreamSynchronize(stream));
             CU(cudaMemcpy(&last_slow, stats, sizeof(last_slow), cudaMemcpyDeviceToHost));
+            check_tc_status();
             stager_.release();
         }
         (void)n;
@@ -1379,6 +1414,7 @@ public:
         if (sync) {
             CU(cudaStreamSynchronize(stream));
             CU(cudaMemcpy(&last_slow, stats, sizeof(last_slow), cudaMemcpyDeviceToHost));
+            check_tc_status();
             stager_.release();
         }
         return BM3D_OK;
@@ -1711,6 +1747,7 @@ BM3D_API int bm3d_synchronize(bm3d_filter *h)
     if (!h) return fail(BM3D_ERR_STATE, "null filter");
     return guarded([&]() {
         CU(cudaStreamSynchronize(h->f->stream));
+        h->f->synced();
         return (int)BM3D_OK;
     });
 }

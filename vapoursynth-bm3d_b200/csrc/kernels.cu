@@ -6,10 +6,15 @@
 #include "bm.cuh"
 #include "vbm.cuh"
 #include "cf.cuh"
+#include "cf_tc.cuh"
 #include "convert.cuh"
 #include "launch.h"
+#include "params.h"
 
+#include <algorithm>
 #include <atomic>
+#include <cstring>
+#include <vector>
 
 namespace bm3d {
 
@@ -80,6 +85,85 @@ cudaError_t launch_cf_fast(const CFArgs &a, int warps, int grid, cudaStream_t s)
     case 16: return w ? launch_cf_fast_t<16, true>(a, warps, grid, s) : launch_cf_fast_t<16, false>(a, warps, grid, s);
     case 32: return w ? launch_cf_fast_t<32, true>(a, warps, grid, s) : launch_cf_fast_t<32, false>(a, warps, grid, s);
     default: return cudaErrorInvalidValue;
+    }
+}
+
+// ---- precision form: tensor-core collaborative filter ------------------------------------------
+
+int cf_tc_supported(int B, int G) { return B == 8 && (G == 8 || G == 16 || G == 32); }
+
+// tf32 value of x, rounded to nearest (ties away), as the tensor cores read it
+static float round_tf32(float x)
+{
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+
+template <int G>
+static void tc_tables_t(std::vector<unsigned char> &img)
+{
+    using Lay = TcLayout<G>;
+    img.assign(Lay::kTableBytes, 0);
+    auto put = [&](uint32_t off, double v) {
+        const float f = round_tf32((float)v);
+        std::memcpy(img.data() + off, &f, 4);
+    };
+    // REDFT10 C[k][j] = 2 cos(pi (j + 1/2) k / N); REDFT01 Ci[j][k] = k == 0 ? 1 : 2 cos(pi k (j + 1/2) / N)
+    auto fwd = [](int N, int k, int j) { return (double)cos2((long)(2 * j + 1) * k, 2L * N); };
+    auto inv = [](int N, int j, int k) { return k == 0 ? 1.0 : (double)cos2((long)k * (2 * j + 1), 2L * N); };
+    const int r0 = 128 - G;                  // rows [r0, r0 + G) of the stacks hold the matrix
+    for (int kz = 0; kz < G; ++kz)
+        for (int jz = 0; jz < G; ++jz) {
+            put(Lay::kZf + tc_kmajor(r0 + kz, jz, G), fwd(G, kz, jz));
+            put(Lay::kZi + tc_kmajor(r0 + jz, kz, G), inv(G, jz, kz));
+        }
+    for (int ky = 0; ky < 8; ++ky)
+        for (int kx = 0; kx < 8; ++kx)
+            for (int y = 0; y < 8; ++y)
+                for (int x = 0; x < 8; ++x) {
+                    const int c = ky * 8 + kx, px = y * 8 + x;
+                    put(Lay::kKf + tc_kmajor(c, px, 64), fwd(8, ky, y) * fwd(8, kx, x));
+                    put(Lay::kKi + tc_kmajor(px, c, 64), inv(8, y, ky) * inv(8, x, kx));
+                }
+}
+
+void cf_tc_tables(int G, std::vector<unsigned char> &img)
+{
+    if (G == 8) tc_tables_t<8>(img);
+    else if (G == 16) tc_tables_t<16>(img);
+    else tc_tables_t<32>(img);
+}
+
+template <int G, bool W>
+static cudaError_t launch_cf_tc_t(const CFArgs &a, const void *tables, int *status, cudaStream_t s)
+{
+    using Shp = TcShape<G, W>;
+    const size_t smem = (size_t)Shp::kSmem;
+    cudaError_t e;
+    if ((e = allow_smem(cf_tc_kernel<G, W>, smem)) != cudaSuccess) return e;
+    int dev = 0, sms = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    // one CTA per SM (shared memory and all 512 tensor-memory columns are taken)
+    const long long ntiles = (a.ngroups + TcLayout<G>::kGroups - 1) / TcLayout<G>::kGroups;
+    const long long grid = std::max<long long>(1, std::min<long long>((ntiles + Shp::kWG - 1) / Shp::kWG, sms));
+    COUNT_LAUNCH();
+    cf_tc_kernel<G, W><<<(unsigned)grid, 128 * Shp::kWG, smem, s>>>(a, static_cast<const float4 *>(tables), ntiles, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cf_tc(const CFArgs &a, const void *tables, int *status, cudaStream_t s)
+{
+    if (!cf_tc_supported(a.B, a.G)) return cudaErrorInvalidValue;
+    const bool w = a.wiener != 0;
+    switch (a.G) {
+    case 8: return w ? launch_cf_tc_t<8, true>(a, tables, status, s) : launch_cf_tc_t<8, false>(a, tables, status, s);
+    case 16: return w ? launch_cf_tc_t<16, true>(a, tables, status, s) : launch_cf_tc_t<16, false>(a, tables, status, s);
+    default: return w ? launch_cf_tc_t<32, true>(a, tables, status, s) : launch_cf_tc_t<32, false>(a, tables, status, s);
     }
 }
 

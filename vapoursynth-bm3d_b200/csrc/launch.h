@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <vector>
 #include "args.h"
 
 namespace bm3d {
@@ -29,6 +31,14 @@ cudaError_t launch_dct3d_test(float *data, int ngroups, int n, int B, int invers
                               cudaStream_t s);
 
 int cf_fast_supported(int B, int G);
+
+// Precision form: collaborative filter of the full groups (n == G) on the tensor cores (tf32
+// transforms); partial groups are left to launch_cf_fast with skip_full = 1.  `tables` is the
+// device copy of the image cf_tc_tables builds for G; *status becomes 1 if a tensor-core wait
+// timed out.
+int cf_tc_supported(int B, int G);
+void cf_tc_tables(int G, std::vector<unsigned char> &img);
+cudaError_t launch_cf_tc(const CFArgs &a, const void *tables, int *status, cudaStream_t s);
 
 // Number of kernels launched by this library since load.
 unsigned long long launch_count();

@@ -1,0 +1,186 @@
+// tc.cuh -- thin wrappers over the sm_100a tensor-core instructions (tcgen05) used by the
+// precision-form kernels: tensor-memory allocation, shared-memory matrix descriptors, the MMA
+// itself (operands in shared memory, or A in tensor memory), commit to an mbarrier, bounded
+// mbarrier waits and tensor-memory loads/stores.
+//
+// Shared-memory operands are K-major (the tf32 kind takes no MN-major operands), either
+//   unswizzled: core matrices of 8 rows x 16 bytes stored as 128 contiguous bytes,
+//     byte(r, k) = (r / 8) * SBO + (k / 4) * LBO + (r % 8) * 16 + (k % 4) * 4   (32-bit elements)
+//     one MMA consumes K = 8, i.e. two core matrices along K; or
+//   128-byte swizzled: atoms of 8 rows x 128 bytes (32 elements of K), see sw128_offset.
+#pragma once
+
+#include <cstdint>
+
+namespace bm3d {
+namespace tc {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor (no swizzle): start address, leading and stride byte offsets
+// (all in 16-byte units), descriptor version 1.
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;      // version
+    return d;                    // base offset 0, lbo mode 0, layout type 0 (no swizzle)
+}
+
+// Same, 128-byte swizzle (K-major only here): atoms of 8 rows x 128 bytes, 1024-byte aligned, the
+// 16-byte chunk index of each row XOR-ed with the row index within the atom.  SBO = stride between
+// 8-row atoms; the K offset inside an atom is added to the start address (multiples of 32 bytes).
+__device__ __forceinline__ uint64_t make_desc_sw128(uint32_t saddr, uint32_t sbo_bytes)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)1 << 16;                       // leading byte offset (unused with swizzling)
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;                       // version
+    d |= (uint64_t)2 << 61;                       // layout type: 128-byte swizzle
+    return d;
+}
+
+// byte offset of element (row, k) of a K-major 32-bit operand with 128-byte swizzle, stored as
+// K-atoms of 32 elements one after the other, each covering all `rows` rows
+__host__ __device__ constexpr uint32_t sw128_offset(int row, int k, int rows)
+{
+    return (uint32_t)((k / 32) * (rows / 8) * 1024 + (row / 8) * 1024 + (row % 8) * 128 +
+                      ((((k % 32) / 4) ^ (row % 8)) * 16) + (k % 4) * 4);
+}
+
+// Instruction descriptor of kind::tf32 with an fp32 accumulator.
+//   a_mn / b_mn: operand is MN-major (1) or K-major (0).
+__host__ __device__ constexpr uint32_t idesc_tf32(int M, int N, int a_mn, int b_mn)
+{
+    return (1u << 4)                    // D format f32
+         | (2u << 7)                    // A format tf32
+         | (2u << 10)                   // B format tf32
+         | ((uint32_t)a_mn << 15)
+         | ((uint32_t)b_mn << 16)
+         | ((uint32_t)(N >> 3) << 17)
+         | ((uint32_t)(M >> 4) << 24);
+}
+
+// ---- tensor memory -------------------------------------------------------------------------------
+
+// Allocates `ncols` columns (power of two >= 32); one full warp executes it.  The address is written
+// to shared memory at `slot`.
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)), "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+}
+
+__device__ __forceinline__ void tmem_free(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols));
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 lanes x 32 bits, 16 consecutive columns per thread: thread t of the warp reads lane
+// (warp's 32-lane quarter) + t.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const float (&v)[16])
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};"
+                 ::"r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+                   "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+                   "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+                   "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+                   "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+                   "r"(__float_as_uint(v[15])));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// ---- MMA -------------------------------------------------------------------------------------------
+
+// D[tmem] (+)= A[smem] * B[smem]; issued by one thread.
+__device__ __forceinline__ void mma_ss_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc, bool accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+                 ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"((uint32_t)accumulate), "r"(0u));
+}
+
+// D[tmem] (+)= A[tmem] * B[smem]; issued by one thread.  A occupies the same lanes as D, K columns.
+__device__ __forceinline__ void mma_ts_tf32(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc, bool accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %5, %5, %5}, p;\n\t}"
+                 ::"r"(d_tmem), "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"((uint32_t)accumulate), "r"(0u));
+}
+
+// Arrives on the mbarrier once every MMA this thread issued before has completed.
+__device__ __forceinline__ void mma_commit(uint64_t *mbar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+
+// ---- named barriers (one per 128-thread warpgroup) ---------------------------------------------------
+
+__device__ __forceinline__ void wg_sync(uint32_t id)
+{
+    asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory");
+}
+
+// barrier of the warpgroup that also ANDs a predicate over its 128 threads
+__device__ __forceinline__ bool wg_and(uint32_t id, bool p)
+{
+    uint32_t r;
+    asm volatile("{\n\t.reg .pred pi, po;\n\tsetp.ne.u32 pi, %1, 0;\n\t"
+                 "bar.red.and.pred po, %2, 128, pi;\n\tselp.u32 %0, 1, 0, po;\n\t}"
+                 : "=r"(r)
+                 : "r"((uint32_t)p), "r"(id)
+                 : "memory");
+    return r != 0;
+}
+
+// ---- mbarrier --------------------------------------------------------------------------------------
+
+__device__ __forceinline__ void mbar_init(uint64_t *mbar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *mbar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(mbar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase with the given parity to complete, giving up after `limit` polls (each poll
+// itself suspends for a hardware-defined time).  Returns false on time-out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *mbar, uint32_t parity, uint32_t limit)
+{
+    for (uint32_t i = 0; i < limit; ++i)
+        if (mbar_try_wait(mbar, parity)) return true;
+    return false;
+}
+
+}  // namespace tc
+}  // namespace bm3d

@@ -187,6 +187,49 @@ __device__ __forceinline__ float lane_combine(const float (&s)[4])
     return __fadd_rn(__fadd_rn(__fadd_rn(s[0], s[1]), s[2]), s[3]);
 }
 
+// Packed pairs of fp32 values (sm_100 f32x2 arithmetic: two IEEE round-to-nearest operations per
+// instruction, each lane exactly as the scalar instruction would round it).  The B = 8 kernel
+// forms the differences and squares of two adjacent columns at once and adds the squares into
+// the four SSE lane sums with scalar adds: the compiler fuses a packed multiply followed by a
+// packed add into one fused multiply-add (single rounding), which would not match the
+// reference's separately rounded square and sum.
+typedef unsigned long long f32x2;
+
+__device__ __forceinline__ f32x2 pack2(float lo, float hi)
+{
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+__device__ __forceinline__ void unpack2(f32x2 v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b)
+{
+    f32x2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b)
+{
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+// acc[2p] += d.lo^2, acc[2p + 1] += d.hi^2 for the column pair p of a row
+__device__ __forceinline__ void add_sq2(float (&acc)[4], int p, f32x2 d)
+{
+    float lo, hi;
+    unpack2(mul2(d, d), lo, hi);
+    acc[2 * p] = __fadd_rn(acc[2 * p], lo);
+    acc[2 * p + 1] = __fadd_rn(acc[2 * p + 1], hi);
+}
+
 template <int BT>
 __global__ void __launch_bounds__(256) bm_full_kernel(BMArgs a)
 {
@@ -246,12 +289,13 @@ __global__ void __launch_bounds__(256) bm_full_kernel(BMArgs a)
     const int ctot = clat + 1;
 
     if constexpr (BT == 8) {
-        float rb[64];
+        // reference block as packed pairs: rbp[y * 4 + m] = (rb[y][2m], rb[y][2m + 1])
+        f32x2 rbp[32];
         const float *rp = win + (j - wy0) * wp + (i - wx0);
 #pragma unroll
         for (int y = 0; y < 8; ++y)
 #pragma unroll
-            for (int x = 0; x < 8; ++x) rb[y * 8 + x] = rp[y * wp + x];
+            for (int m = 0; m < 4; ++m) rbp[y * 4 + m] = pack2(rp[y * wp + 2 * m], rp[y * wp + 2 * m + 1]);
 
         const int nq = (ncols + 3) >> 2;
         const int items = nrows * nq;
@@ -272,18 +316,20 @@ __global__ void __launch_bounds__(256) bm_full_kernel(BMArgs a)
                     float w[11];
 #pragma unroll
                     for (int k = 0; k < 11; ++k) w[k] = wr[y * wp + k];
+                    // window pairs starting at even (E) and odd (O) columns
+                    f32x2 E[5], O[5];
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) {
+                        E[m] = pack2(w[2 * m], w[2 * m + 1]);
+                        O[m] = pack2(w[2 * m + 1], w[2 * m + 2]);
+                    }
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
+                        const f32x2 *Wp = (u & 1) ? O : E;
+                        const int m0 = u >> 1;
+                        // columns 0..3 (lane k takes column k), then 4..7 (lane k takes 4 + k)
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const float d = __fsub_rn(rb[y * 8 + k], w[u + k]);
-                            acc[u][k] = __fadd_rn(acc[u][k], __fmul_rn(d, d));
-                        }
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const float d = __fsub_rn(rb[y * 8 + 4 + k], w[u + 4 + k]);
-                            acc[u][k] = __fadd_rn(acc[u][k], __fmul_rn(d, d));
-                        }
+                        for (int h = 0; h < 4; ++h) add_sq2(acc[u], h & 1, sub2(rbp[y * 4 + h], Wp[m0 + h]));
                     }
                 }
             } else {
@@ -294,15 +340,8 @@ __global__ void __launch_bounds__(256) bm_full_kernel(BMArgs a)
 #pragma unroll
                     for (int y = 0; y < 8; ++y) {
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const float d = __fsub_rn(rb[y * 8 + k], wu[y * wp + k]);
-                            acc[u][k] = __fadd_rn(acc[u][k], __fmul_rn(d, d));
-                        }
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const float d = __fsub_rn(rb[y * 8 + 4 + k], wu[y * wp + 4 + k]);
-                            acc[u][k] = __fadd_rn(acc[u][k], __fmul_rn(d, d));
-                        }
+                        for (int h = 0; h < 4; ++h)
+                            add_sq2(acc[u], h & 1, sub2(rbp[y * 4 + h], pack2(wu[y * wp + 2 * h], wu[y * wp + 2 * h + 1])));
                     }
                 }
             }
@@ -318,15 +357,7 @@ __global__ void __launch_bounds__(256) bm_full_kernel(BMArgs a)
             for (int y = 0; y < 8; ++y) {
                 const float *g = plane + (long long)y * a.ld;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const float d = __fsub_rn(rb[y * 8 + k], __ldg(g + k));
-                    acc[k] = __fadd_rn(acc[k], __fmul_rn(d, d));
-                }
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const float d = __fsub_rn(rb[y * 8 + 4 + k], __ldg(g + 4 + k));
-                    acc[k] = __fadd_rn(acc[k], __fmul_rn(d, d));
-                }
+                for (int h = 0; h < 4; ++h) add_sq2(acc, h & 1, sub2(rbp[y * 4 + h], pack2(__ldg(g + 2 * h), __ldg(g + 2 * h + 1))));
             }
             sd[clat] = lane_combine(acc);
         }

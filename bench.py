@@ -389,6 +389,8 @@ def ours_arm(args):
             return float(G), 1.0
         return float(cnt.mean()), float((cnt == G).mean())
 
+    for st in (pipe.basic, pipe.final):
+        L.bm3d_synchronize(st.h)
     (nb_mean, nb_full), (nf_mean, nf_full) = mean_n(pipe.basic, 16, nb_b), mean_n(pipe.final, 32, nb_f)
     bm_b, dct_b, _ = algorithmic_work(Wd, Hd, F, 4, 16, nb_mean, False)
     bm_f, dct_f, _ = algorithmic_work(Wd, Hd, F, 3, 32, nf_mean, True)
@@ -440,7 +442,9 @@ def ours_arm(args):
                     "d2h_bytes_per_step": int(nz.nbytes), "ms_per_step": round(R["ms_e2e"], 3)},
             "ms_per_step_unprofiled": round(R["ms_unprofiled"], 3),
             "groups": {"basic_mean_n": round(nb_mean, 3), "basic_full_fraction": round(nb_full, 4),
-                       "final_mean_n": round(nf_mean, 3), "final_full_fraction": round(nf_full, 4)},
+                       "final_mean_n": round(nf_mean, 3), "final_full_fraction": round(nf_full, 4),
+                       "basic_exact_tie_blocks": int(L.bm3d_debug_slow_blocks(pipe.basic.h)),
+                       "final_exact_tie_blocks": int(L.bm3d_debug_slow_blocks(pipe.final.h))},
             "gpu_launches": int(R["launches"]),
             "clocks": clk,
             "quality": {"psnr_in_db": round(psnr_in, 3), "psnr_out_db": round(R["psnr"], 3)},

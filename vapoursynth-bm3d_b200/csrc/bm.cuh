@@ -60,10 +60,15 @@ __device__ void select_and_emit(float *sd, int ctot, uint32_t *list, float *hk, 
     uint32_t *opos = a.out_pos + ob * G;
     float *okey = a.out_key ? a.out_key + ob * G : nullptr;
 
-    // count valid candidates and keep each lane's two best (dist, index) composites
+    // count valid candidates and keep each lane's two best (dist, index) composites.  Lane l
+    // takes element (l + 7 k) mod 32 of round k: with the plain stride the best candidates of a
+    // smooth window (a compact patch around the reference position) fall on few lanes, so that
+    // two per lane would often not cover the top group_size
     int cnt = 0;
     uint64_t b1 = ~0ull, b2 = ~0ull;
-    for (int c = lane; c < ctot; c += 32) {
+    for (int c0 = 0; c0 < ctot; c0 += 32) {
+        const int c = c0 + ((lane + 7 * (c0 >> 5)) & 31);
+        if (c >= ctot) continue;
         const float d = sd[c];
         if (dist_valid(d, a.thSSE)) {
             ++cnt;
@@ -297,11 +302,13 @@ __global__ void __launch_bounds__(256) bm_full_kernel(BMArgs a)
 #pragma unroll
             for (int m = 0; m < 4; ++m) rbp[y * 4 + m] = pack2(rp[y * wp + 2 * m], rp[y * wp + 2 * m + 1]);
 
+        // item = 4 horizontally adjacent candidates; consecutive lanes take consecutive rows of
+        // the same quad column (with the odd window pitch their loads hit distinct banks)
         const int nq = (ncols + 3) >> 2;
         const int items = nrows * nq;
         for (int it = lane; it < items; it += 32) {
-            const int ry = it / nq;
-            const int q = it - ry * nq;
+            const int q = it / nrows;
+            const int ry = it - q * nrows;
             const int cy = t + ry * s;
             const int cx0 = l + 4 * q * s;
             float acc[4][4];

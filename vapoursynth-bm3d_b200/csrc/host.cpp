@@ -885,7 +885,11 @@ public:
         return BM3D_OK;
     }
 
-    void synced() override { check_tc_status(); }
+    void synced() override
+    {
+        CU(cudaMemcpy(&last_slow, stats, sizeof(last_slow), cudaMemcpyDeviceToHost));
+        check_tc_status();
+    }
 
     // time-out flag of the tensor-core kernel (read after the stream is synchronised)
     void check_tc_status()
@@ -996,7 +1000,9 @@ public:
         int warps = 8;
         for (; warps >= 1; warps /= 2) {
             a.warps = warps;
-            a.win_pitch = std::min(W, (warps - 1) * para.step + 2 * a.range + a.B) + 4;
+            // odd pitch: the lanes of a warp read consecutive window rows, which then fall in
+            // distinct shared-memory banks
+            a.win_pitch = (std::min(W, (warps - 1) * para.step + 2 * a.range + a.B) + 4) | 1;
             smem = sizeof(float) * ((size_t)a.win_h * a.win_pitch + (size_t)warps * bm_warp_floats(a.cand_cap, a.G, a.B, a.B != 8));
             if (smem <= 200 * 1024) break;
         }

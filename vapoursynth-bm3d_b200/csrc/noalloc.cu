@@ -248,7 +248,7 @@ extern "C" BM3D_API int bm3d_basic_noalloc(const float *src, float *dst, int wid
     int warps = 8;
     for (; warps >= 1; warps /= 2) {
         ba.warps = warps;
-        ba.win_pitch = std::min(width, (warps - 1) * para.step + 2 * ba.range + B) + 4;
+        ba.win_pitch = (std::min(width, (warps - 1) * para.step + 2 * ba.range + B) + 4) | 1;
         smem = sizeof(float) * ((size_t)ba.win_h * ba.win_pitch + (size_t)warps * bm_warp_floats(ba.cand_cap, G, B, false));
         if (smem <= 200 * 1024) break;
     }

@@ -13,16 +13,17 @@
 // so that one warpgroup's gathers and atomics overlap another's tensor-core work; the DCT tables
 // are shared.  Every shared-memory operand is K-major (the tf32 kind takes no MN-major operands):
 //   1. gather  X[b][pixel] (A operand, 128-byte swizzle); Final also gathers the reference group
-//      R.  A warp loads one block per step (lane = pixel row / column), so each load touches the
-//      block's own 4 rows instead of 32 blocks; the block origins come from the owning lanes by
-//      shuffles
+//      R.  A warp copies one block per step (lane = pixel row / column) with asynchronous
+//      global -> shared copies, so each instruction touches the block's own 4 rows instead of 32
+//      blocks and no register waits for the data; the block origins come from the owning lanes
+//      by shuffles
 //   2. 2-D DCT Y = X . K2 into tensor memory cols [0, 64) (ref [64, 128))
 //   3. transpose: each thread reads its row of Y and writes it as column b of Yt[coef][b], a B
 //      operand with 128-byte swizzle (conflict-free column writes); Final stacks the reference
 //      coefficients below (rows 64..127), so one N = 128 product transforms both
-//   4. z-DCT   Z = Zf_w . Yt_w per group w into cols [0, 64) (ref [64, 128)); the A operand
-//      Zf_w is a 128-row window of a zero-padded stack around one copy of the G x G DCT matrix,
-//      so that group w lands in rows [G w, G w + G)
+//   4. z-DCT   Z = Zf . Yt_w per group w into cols [0, 64) (ref [64, 128)); the A operand Zf
+//      stacks 128 / G copies of the G x G DCT matrix and every output lane outside group w's rows
+//      [G w, G w + G) is disabled in that product
 //   5. shrink  thread r owns row (group, z-frequency) of 64 coefficients: hard threshold (Basic)
 //      or Wiener weights from the reference spectrum (Final); the group's count / L2 is a
 //      reduction over its G lanes; S goes back to shared memory as St[coef][kz] (swizzled B)
@@ -45,7 +46,7 @@ namespace bm3d {
 template <int G>
 struct TcLayout {
     static constexpr int kGroups = 128 / G;            // groups per tile
-    static constexpr int kZRows = 256 - G;             // zero-padded stack of the G x G DCT matrix
+    static constexpr int kZRows = 128;                 // 128 / G stacked copies of the G x G DCT matrix
     static constexpr int kZBytes = kZRows * G * 4;
     static constexpr int kKBytes = 64 * 64 * 4;
     static constexpr int kZf = 0;                       // forward z matrix stack (K-major)
@@ -56,13 +57,19 @@ struct TcLayout {
     static constexpr int kXBytes = 128 * 64 * 4;        // one 128 x 64 data operand
 };
 
-// warpgroups per CTA: shared memory holds the tables and, per warpgroup, one (Basic) or two
-// (Final) 32 KB operands; tensor memory gives 128 columns to each of at most 4
+// Tile teams per CTA: shared memory holds the tables and, per team, one (Basic) or two (Final)
+// 32 KB operands; tensor memory gives 128 columns to each of at most 4.  A team is one warp per
+// 32-row quarter of the tile (kSplit = 1) or two (kSplit = 2: the two warps of a quarter share its
+// columns and gather / aggregation steps), so that the Final kernel, limited to two teams by
+// shared memory, still runs 16 warps per SM.
 template <int G, bool WIENER>
 struct TcShape {
     static constexpr int kWG = WIENER ? 2 : 4;
+    static constexpr int kSplit = WIENER ? 2 : 1;
+    static constexpr int kTeam = 128 * kSplit;          // threads per team
     static constexpr int kData = TcLayout<G>::kXBytes * (WIENER ? 2 : 1);
-    static constexpr int kSmem = kData * kWG + TcLayout<G>::kTableBytes;
+    static constexpr int kPart = WIENER ? kTeam * 4 : 0; // per-row partial sums of the two halves
+    static constexpr int kSmem = (kData + kPart) * kWG + TcLayout<G>::kTableBytes;
 };
 
 // byte offset of element (row, k) of a K-major operand with `kdim` columns
@@ -74,31 +81,39 @@ __host__ __device__ constexpr uint32_t tc_kmajor(int row, int k, int kdim)
 constexpr uint32_t kTcWaitLimit = 1u << 24;
 
 template <int G, bool WIENER>
-__global__ void __launch_bounds__(128 * TcShape<G, WIENER>::kWG, 1)
+__global__ void __launch_bounds__(TcShape<G, WIENER>::kTeam * TcShape<G, WIENER>::kWG, 1)
 cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
 {
     using Lay = TcLayout<G>;
     using Shp = TcShape<G, WIENER>;
     constexpr int GPT = Lay::kGroups;
     constexpr int NWG = Shp::kWG;
+    constexpr int SPLIT = Shp::kSplit;
+    constexpr int TEAM = Shp::kTeam;
+    constexpr int NC = 64 / SPLIT;                   // columns per thread in the row phases
+    constexpr int NI = 32 / SPLIT;                   // blocks per warp in the block-step phases
     constexpr int NT = WIENER ? 128 : 64;            // rows of the z-stage B operand
     extern __shared__ __align__(1024) unsigned char tsm[];
     __shared__ __align__(8) uint64_t mbar[NWG];
     __shared__ uint32_t tslot;
 
-    const int wg = threadIdx.x >> 7;
-    const int r = threadIdx.x & 127;                 // row of the tile
+    const int wg = threadIdx.x / TEAM;
+    const int t = threadIdx.x % TEAM;
+    const int r = t & 127;                           // row of the tile (tensor-memory lane)
+    const int half = t >> 7;                         // column half (SPLIT = 2)
+    const int cb = half * NC;                        // first column of this thread
     const int warp = threadIdx.x >> 5;
     const uint32_t bar_id = 1 + wg;
     const int wsub = r / G;                          // group within the tile
     const int j = r % G;                             // block index in the group / z-frequency
     unsigned char *D = tsm + Shp::kData * wg;        // X | R, then Yt, then St
-    unsigned char *tab = tsm + Shp::kData * NWG;
+    float *part = reinterpret_cast<float *>(tsm + Shp::kData * NWG + Shp::kPart * wg);
+    unsigned char *tab = tsm + (Shp::kData + Shp::kPart) * NWG;
 
     for (int i = threadIdx.x; i < Lay::kTableBytes / 16; i += blockDim.x)
         reinterpret_cast<float4 *>(tab)[i] = tables[i];
     if (warp == 0) tc::tmem_alloc(&tslot, 128 * NWG);
-    if (r == 0) tc::mbar_init(&mbar[wg], 1);
+    if (t == 0) tc::mbar_init(&mbar[wg], 1);
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
@@ -118,12 +133,12 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
         const bool ok = tc::mbar_wait_bounded(mb, phase, kTcWaitLimit);
         phase ^= 1u;
         tc::fence_after_sync();
-        return tc::wg_and(bar_id, ok);
+        return tc::wg_and(bar_id, TEAM, ok);
     };
     auto publish = [&]() {
         tc::fence_proxy_async_smem();
         tc::fence_before_sync();
-        tc::wg_sync(bar_id);
+        tc::wg_sync(bar_id, TEAM);
         tc::fence_after_sync();
     };
     // 2-D stage, A in shared memory: D[d0, +64) = X . K (X swizzled [128][64], K [64 n][64 k])
@@ -139,27 +154,36 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
         for (int s = 0; s < 8; ++s)
             tc::mma_ts_tf32(tb + d0, tb + a0 + 8 * s, tc::make_desc(sk + s * 256, 128, 2048), ID64, s > 0);
     };
-    // z stage: D[d0, +nt) = sum_w Zwin_w . Bt_w, Bt swizzled [nt rows][128 k], K range of group w
+    // z stage: rows of group w of D[d0, +nt) = Zstack . Bt_w (K range of group w), every other
+    // output lane disabled; Bt swizzled [nt rows][128 k]
     auto z_stage = [&](uint32_t d0, uint32_t sz, int nt, uint32_t idesc) {
 #pragma unroll 1
-        for (int w = 0; w < GPT; ++w)
+        for (int w = 0; w < GPT; ++w) {
+            uint32_t m[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int lo = G * w - 32 * q, hi = lo + G;      // enabled lanes of word q: [lo, hi)
+                const uint32_t en = (hi <= 0 || lo >= 32) ? 0u
+                                  : (G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lo < 0 ? 0 : lo)));
+                m[q] = ~en;
+            }
 #pragma unroll 1
             for (int s = 0; s < G / 8; ++s) {
-                const uint32_t arow = (uint32_t)((128 - G) - G * w);
-                const uint64_t ad = tc::make_desc(sz + (arow / 8) * (G / 4) * 128 + s * 256, 128, (G / 4) * 128);
+                const uint64_t ad = tc::make_desc(sz + s * 256, 128, (G / 4) * 128);
                 const uint32_t k0 = (uint32_t)(G * w + 8 * s);
                 const uint64_t bd = tc::make_desc_sw128(sD + (k0 / 32) * (nt / 8) * 1024 + ((k0 % 32) / 8) * 32, 1024);
-                tc::mma_ss_tf32(tb + d0, ad, bd, idesc, !(w == 0 && s == 0));
+                tc::mma_ss_tf32_masked(tb + d0, ad, bd, idesc, s > 0, m[0], m[1], m[2], m[3]);
             }
+        }
     };
-    // this thread's row of tensor memory (cols c0..c0+63) -> column r, rows row0.., of Bt
+    // this thread's columns of its tensor-memory row (c0 + cb ..) -> column r, rows row0 + cb .., of Bt
     auto row_to_column = [&](uint32_t c0, int row0, int nt) {
-        float v[64];
+        float v[NC];
 #pragma unroll
-        for (int q = 0; q < 64; q += 16) tc::tmem_ld16(tb + lrow + c0 + q, *reinterpret_cast<float (*)[16]>(v + q));
+        for (int q = 0; q < NC; q += 16) tc::tmem_ld16(tb + lrow + c0 + cb + q, *reinterpret_cast<float (*)[16]>(v + q));
         tc::tmem_wait_ld();
 #pragma unroll
-        for (int e = 0; e < 64; ++e) *reinterpret_cast<float *>(D + tc::sw128_offset(row0 + e, r, nt)) = v[e];
+        for (int e = 0; e < NC; ++e) *reinterpret_cast<float *>(D + tc::sw128_offset(row0 + cb + e, r, nt)) = v[e];
     };
 
     bool failed = false;
@@ -180,31 +204,34 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
                 const int b0 = r & ~31;
 #pragma unroll 4
-                for (int i = 0; i < 32; ++i) {
+                for (int i = half * NI; i < half * NI + NI; ++i) {
                     const bool mi = __shfl_sync(0xffffffffu, mine, i);
                     const float *si = reinterpret_cast<const float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(sp), i));
-                    float v0 = 0.f, v1 = 0.f;
+                    unsigned char *d0 = D + tc::sw128_offset(b0 + i, lane, 128);
+                    unsigned char *d1 = D + tc::sw128_offset(b0 + i, lane + 32, 128);
                     if (mi) {
-                        v0 = __ldg(si + (long long)ry * a.ld + cx);
-                        v1 = __ldg(si + (long long)(ry + 4) * a.ld + cx);
+                        tc::cp_async4(d0, si + (long long)ry * a.ld + cx);
+                        tc::cp_async4(d1, si + (long long)(ry + 4) * a.ld + cx);
+                    } else {
+                        *reinterpret_cast<float *>(d0) = 0.0f;
+                        *reinterpret_cast<float *>(d1) = 0.0f;
                     }
-                    *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128)) = v0;
-                    *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
                     if constexpr (WIENER) {
                         const float *ri = reinterpret_cast<const float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(rp), i));
-                        float u0 = 0.f, u1 = 0.f;
                         if (mi) {
-                            u0 = __ldg(ri + (long long)ry * a.ld + cx);
-                            u1 = __ldg(ri + (long long)(ry + 4) * a.ld + cx);
+                            tc::cp_async4(d0 + Lay::kXBytes, ri + (long long)ry * a.ld + cx);
+                            tc::cp_async4(d1 + Lay::kXBytes, ri + (long long)(ry + 4) * a.ld + cx);
+                        } else {
+                            *reinterpret_cast<float *>(d0 + Lay::kXBytes) = 0.0f;
+                            *reinterpret_cast<float *>(d1 + Lay::kXBytes) = 0.0f;
                         }
-                        *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128)) = u0;
-                        *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane + 32, 128)) = u1;
                     }
                 }
+                tc::cp_async_wait_all();
             }
             publish();
             // 2. 2-D DCT
-            if (r == 0) {
+            if (t == 0) {
                 xy_ss(0, sD, sKf);
                 if constexpr (WIENER) xy_ss(64, sD + Lay::kXBytes, sKf);
                 tc::mma_commit(mb);
@@ -215,22 +242,25 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             if constexpr (WIENER) row_to_column(64, 64, NT);
             publish();
             // 4. z-DCT of source (and reference) in one pass
-            if (r == 0) {
+            if (t == 0) {
                 z_stage(0, sZf, NT, IDZ);
                 tc::mma_commit(mb);
             }
             if (!wait_mma()) { failed = true; break; }
             // 5. shrinkage, one row of 64 coefficients per thread
             float acc = 0.0f;
+            float thr[3];                              // by the number of zero (y, x) frequencies
 #pragma unroll
-            for (int c0 = 0; c0 < 64; c0 += 32) {
+            for (int k = 0; k < 3; ++k) thr[k] = WIENER ? 0.0f : a.thr4[p][G - 1][(j == 0) + k];
+#pragma unroll
+            for (int c0 = 0; c0 < NC; c0 += 32) {
                 float z[32];
-                tc::tmem_ld16(tb + lrow + c0, *reinterpret_cast<float (*)[16]>(z));
-                tc::tmem_ld16(tb + lrow + c0 + 16, *reinterpret_cast<float (*)[16]>(z + 16));
+                tc::tmem_ld16(tb + lrow + cb + c0, *reinterpret_cast<float (*)[16]>(z));
+                tc::tmem_ld16(tb + lrow + cb + c0 + 16, *reinterpret_cast<float (*)[16]>(z + 16));
                 if constexpr (WIENER) {
                     float rr[32];
-                    tc::tmem_ld16(tb + lrow + 64 + c0, *reinterpret_cast<float (*)[16]>(rr));
-                    tc::tmem_ld16(tb + lrow + 64 + c0 + 16, *reinterpret_cast<float (*)[16]>(rr + 16));
+                    tc::tmem_ld16(tb + lrow + 64 + cb + c0, *reinterpret_cast<float (*)[16]>(rr));
+                    tc::tmem_ld16(tb + lrow + 64 + cb + c0 + 16, *reinterpret_cast<float (*)[16]>(rr + 16));
                     tc::tmem_wait_ld();
                     const float sg = a.wsig2[p][G - 1];
 #pragma unroll
@@ -244,18 +274,23 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     tc::tmem_wait_ld();
 #pragma unroll
                     for (int e = 0; e < 32; ++e) {
-                        const int c = c0 + e;
-                        const int flag = (j == 0) + ((c & 7) == 0) + ((c >> 3) == 0);
-                        const bool keep = fabsf(z[e]) > a.thr4[p][G - 1][flag];
+                        const int c = cb + c0 + e;
+                        const bool keep = fabsf(z[e]) > thr[((c & 7) == 0) + ((c >> 3) == 0)];
                         acc += keep ? 1.0f : 0.0f;
                         z[e] = keep ? z[e] : 0.0f;
                     }
                 }
 #pragma unroll
-                for (int e = 0; e < 32; ++e) *reinterpret_cast<float *>(D + tc::sw128_offset(c0 + e, r, 64)) = z[e];
+                for (int e = 0; e < 32; ++e) *reinterpret_cast<float *>(D + tc::sw128_offset(cb + c0 + e, r, 64)) = z[e];
             }
 #pragma unroll
             for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if constexpr (SPLIT == 2) {
+                // the group's sum is the sum of the two column halves
+                part[t] = acc;
+                tc::wg_sync(bar_id, TEAM);
+                acc = part[r] + part[r + 128];
+            }
             float denW;
             if constexpr (WIENER) {
                 const float eps = 1.1920928955078125e-07f;
@@ -266,31 +301,32 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             const float numW = denW / a.amp[G - 1];
             publish();
             // 6. inverse z, then inverse 2-D
-            if (r == 0) {
+            if (t == 0) {
                 z_stage(0, sZi, 64, ID64);
                 tc::mma_commit(mb);
             }
             if (!wait_mma()) { failed = true; break; }
-            if (r == 0) {
+            if (t == 0) {
                 xy_ts(64, 0, sKi);
                 tc::mma_commit(mb);
             }
             if (!wait_mma()) { failed = true; break; }
-            // 7. aggregation: rows -> shared memory (this warp's 32 rows), then one block per step
+            // 7. aggregation: rows -> shared memory (this quarter's 32 rows), then one block per step
             {
-                float v[64];
+                float v[NC];
 #pragma unroll
-                for (int c0 = 0; c0 < 64; c0 += 16) tc::tmem_ld16(tb + lrow + 64 + c0, *reinterpret_cast<float (*)[16]>(v + c0));
+                for (int c0 = 0; c0 < NC; c0 += 16) tc::tmem_ld16(tb + lrow + 64 + cb + c0, *reinterpret_cast<float (*)[16]>(v + c0));
                 tc::tmem_wait_ld();
 #pragma unroll
-                for (int c = 0; c < 64; c += 4)
-                    *reinterpret_cast<float4 *>(D + tc::sw128_offset(r, c, 128)) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
-                __syncwarp();
+                for (int c = 0; c < NC; c += 4)
+                    *reinterpret_cast<float4 *>(D + tc::sw128_offset(r, cb + c, 128)) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+                if constexpr (SPLIT == 2) tc::wg_sync(bar_id, TEAM);
+                else __syncwarp();
                 float *np = L.num + (long long)L.y * a.ld + L.x;
                 const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
                 const int b0 = r & ~31;
 #pragma unroll 4
-                for (int i = 0; i < 32; ++i) {
+                for (int i = half * NI; i < half * NI + NI; ++i) {
                     const bool mi = __shfl_sync(0xffffffffu, mine, i);
                     float *ni = reinterpret_cast<float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(np), i));
                     const float wi = __shfl_sync(0xffffffffu, numW, i);
@@ -302,13 +338,13 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     }
                 }
             }
-            if (mine) atomicAdd(L.wmap + (long long)L.y * a.ld + L.x, denW);
+            if (mine && half == 0) atomicAdd(L.wmap + (long long)L.y * a.ld + L.x, denW);
             tc::fence_before_sync();
-            tc::wg_sync(bar_id);
+            tc::wg_sync(bar_id, TEAM);
             tc::fence_after_sync();
         }
     }
-    if (failed && r == 0) atomicExch(status, 1);
+    if (failed && t == 0) atomicExch(status, 1);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();

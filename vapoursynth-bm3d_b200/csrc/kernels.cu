@@ -115,12 +115,12 @@ static void tc_tables_t(std::vector<unsigned char> &img)
     // REDFT10 C[k][j] = 2 cos(pi (j + 1/2) k / N); REDFT01 Ci[j][k] = k == 0 ? 1 : 2 cos(pi k (j + 1/2) / N)
     auto fwd = [](int N, int k, int j) { return (double)cos2((long)(2 * j + 1) * k, 2L * N); };
     auto inv = [](int N, int j, int k) { return k == 0 ? 1.0 : (double)cos2((long)k * (2 * j + 1), 2L * N); };
-    const int r0 = 128 - G;                  // rows [r0, r0 + G) of the stacks hold the matrix
-    for (int kz = 0; kz < G; ++kz)
-        for (int jz = 0; jz < G; ++jz) {
-            put(Lay::kZf + tc_kmajor(r0 + kz, jz, G), fwd(G, kz, jz));
-            put(Lay::kZi + tc_kmajor(r0 + jz, kz, G), inv(G, jz, kz));
-        }
+    for (int w = 0; w < 128 / G; ++w)        // one copy of the matrices per group of a tile
+        for (int kz = 0; kz < G; ++kz)
+            for (int jz = 0; jz < G; ++jz) {
+                put(Lay::kZf + tc_kmajor(G * w + kz, jz, G), fwd(G, kz, jz));
+                put(Lay::kZi + tc_kmajor(G * w + jz, kz, G), inv(G, jz, kz));
+            }
     for (int ky = 0; ky < 8; ++ky)
         for (int kx = 0; kx < 8; ++kx)
             for (int y = 0; y < 8; ++y)
@@ -152,7 +152,7 @@ static cudaError_t launch_cf_tc_t(const CFArgs &a, const void *tables, int *stat
     const long long ntiles = (a.ngroups + TcLayout<G>::kGroups - 1) / TcLayout<G>::kGroups;
     const long long grid = std::max<long long>(1, std::min<long long>((ntiles + Shp::kWG - 1) / Shp::kWG, sms));
     COUNT_LAUNCH();
-    cf_tc_kernel<G, W><<<(unsigned)grid, 128 * Shp::kWG, smem, s>>>(a, static_cast<const float4 *>(tables), ntiles, status);
+    cf_tc_kernel<G, W><<<(unsigned)grid, Shp::kTeam * Shp::kWG, smem, s>>>(a, static_cast<const float4 *>(tables), ntiles, status);
     return cudaGetLastError();
 }
 

@@ -123,6 +123,17 @@ __device__ __forceinline__ void mma_ss_tf32(uint32_t d_tmem, uint64_t a_desc, ui
                  ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"((uint32_t)accumulate), "r"(0u));
 }
 
+// Same, with the output lanes whose bit is set in (m0, m1, m2, m3) (lane i: bit i % 32 of word
+// i / 32) left untouched.
+__device__ __forceinline__ void mma_ss_tf32_masked(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                                   bool accumulate, uint32_t m0, uint32_t m1, uint32_t m2, uint32_t m3)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                 ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"((uint32_t)accumulate),
+                   "r"(m0), "r"(m1), "r"(m2), "r"(m3));
+}
+
 // D[tmem] (+)= A[tmem] * B[smem]; issued by one thread.  A occupies the same lanes as D, K columns.
 __device__ __forceinline__ void mma_ts_tf32(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc, bool accumulate)
 {
@@ -137,21 +148,33 @@ __device__ __forceinline__ void mma_commit(uint64_t *mbar)
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar)) : "memory");
 }
 
-// ---- named barriers (one per 128-thread warpgroup) ---------------------------------------------------
+// ---- asynchronous global -> shared copies (no register round trip) --------------------------------
 
-__device__ __forceinline__ void wg_sync(uint32_t id)
+__device__ __forceinline__ void cp_async4(void *smem_dst, const float *gsrc)
 {
-    asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_u32(smem_dst)), "l"(gsrc) : "memory");
 }
 
-// barrier of the warpgroup that also ANDs a predicate over its 128 threads
-__device__ __forceinline__ bool wg_and(uint32_t id, bool p)
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// ---- named barriers (one per tile team of threads) ---------------------------------------------------
+
+__device__ __forceinline__ void wg_sync(uint32_t id, uint32_t nthreads)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// barrier of `nthreads` threads that also ANDs a predicate over them
+__device__ __forceinline__ bool wg_and(uint32_t id, uint32_t nthreads, bool p)
 {
     uint32_t r;
     asm volatile("{\n\t.reg .pred pi, po;\n\tsetp.ne.u32 pi, %1, 0;\n\t"
-                 "bar.red.and.pred po, %2, 128, pi;\n\tselp.u32 %0, 1, 0, po;\n\t}"
+                 "bar.red.and.pred po, %2, %3, pi;\n\tselp.u32 %0, 1, 0, po;\n\t}"
                  : "=r"(r)
-                 : "r"((uint32_t)p), "r"(id)
+                 : "r"((uint32_t)p), "r"(id), "r"(nthreads)
                  : "memory");
     return r != 0;
 }

@@ -30,8 +30,10 @@
 //   6. inverse z into cols [0, 64), then inverse 2-D with A read from tensor memory into
 //      cols [64, 128)
 //   7. aggregate: the inverse rows go through shared memory so that a warp adds one block per
-//      step with lane = pixel (one 32-byte sector per block row and atomic instruction instead of
-//      32 scattered sectors); the block weight goes to the weight map as in the plain kernel.
+//      step with lane = pixel; in region mode into the staged region (fixed-point integer
+//      atomics, then one pass of vector atomics to the numerator plane), otherwise straight to the
+//      numerator plane (one 32-byte sector per block row and atomic instruction instead of 32
+//      scattered sectors); the block weight goes to the weight map as in the plain kernel.
 // Every wait on the tensor cores is bounded; on time-out the warpgroup records the failure in
 // *status and stops; the CTA releases its tensor memory and returns.
 #pragma once
@@ -60,16 +62,19 @@ struct TcLayout {
 // Tile teams per CTA: shared memory holds the tables and, per team, one (Basic) or two (Final)
 // 32 KB operands; tensor memory gives 128 columns to each of at most 4.  A team is one warp per
 // 32-row quarter of the tile (kSplit = 1) or two (kSplit = 2: the two warps of a quarter share its
-// columns and gather / aggregation steps), so that the Final kernel, limited to two teams by
-// shared memory, still runs 16 warps per SM.
+// columns and gather / aggregation steps), so that the kernels limited to two teams by shared
+// memory (Final, and Basic with G = 32) still run 16 warps per SM.
 template <int G, bool WIENER>
 struct TcShape {
-    static constexpr int kWG = WIENER ? 2 : 4;
-    static constexpr int kSplit = WIENER ? 2 : 1;
+    static constexpr bool kTwo = WIENER || G == 32;     // two teams (shared memory), split quarters
+    static constexpr int kWG = kTwo ? 2 : 4;
+    static constexpr int kSplit = kTwo ? 2 : 1;
     static constexpr int kTeam = 128 * kSplit;          // threads per team
     static constexpr int kData = TcLayout<G>::kXBytes * (WIENER ? 2 : 1);
-    static constexpr int kPart = WIENER ? kTeam * 4 : 0; // per-row partial sums of the two halves
-    static constexpr int kSmem = (kData + kPart) * kWG + TcLayout<G>::kTableBytes;
+    static constexpr int kPart = kSplit == 2 ? kTeam * 4 : 0; // per-row partial sums of the two halves
+    static constexpr int kRegion = 3072;                  // floats of the staged image region
+    static constexpr int kExtra = kPart + kRegion * 4 + 128;   // + [4 quarters][8] ints of bounds
+    static constexpr int kSmem = (kData + kExtra) * kWG + TcLayout<G>::kTableBytes;
 };
 
 // byte offset of element (row, k) of a K-major operand with `kdim` columns
@@ -107,8 +112,11 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     const int wsub = r / G;                          // group within the tile
     const int j = r % G;                             // block index in the group / z-frequency
     unsigned char *D = tsm + Shp::kData * wg;        // X | R, then Yt, then St
-    float *part = reinterpret_cast<float *>(tsm + Shp::kData * NWG + Shp::kPart * wg);
-    unsigned char *tab = tsm + (Shp::kData + Shp::kPart) * NWG;
+    unsigned char *extra = tsm + Shp::kData * NWG + Shp::kExtra * wg;
+    float *part = reinterpret_cast<float *>(extra);
+    float *Rg = reinterpret_cast<float *>(extra + Shp::kPart);         // staged region / accumulator
+    int *bbx = reinterpret_cast<int *>(extra + Shp::kPart + Shp::kRegion * 4);   // [4 quarters][8]
+    unsigned char *tab = tsm + (Shp::kData + Shp::kExtra) * NWG;
 
     for (int i = threadIdx.x; i < Lay::kTableBytes / 16; i += blockDim.x)
         reinterpret_cast<float4 *>(tab)[i] = tables[i];
@@ -197,12 +205,81 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
         for (int p = 0; p < 3 && !failed; ++p) {
             if (!a.process[p]) continue;
             const GroupLoc L = locate(a, p, g0, pk);
-            // 1. gather (rows of foreign or partial groups are zero), one block per warp step
+            const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
+            const int b0 = r & ~31;
+            // Region mode (BM3D): every full group of the tile lies in one frame and the bounding
+            // box of its blocks fits the region buffer; the box is then staged once with aligned
+            // 16-byte copies and the blocks are cut out of shared memory, and the aggregation adds
+            // into the same buffer before one pass of vector atomics.  Otherwise blocks are copied
+            // and added one by one.
+            int y0 = 0, x0 = 0, rh = 0, rw = 0, frame = 0;
+            bool region = false;
             {
+                const long long f = g0 / a.blocks_per_frame;
+                int ymin = mine ? L.y : 1 << 30, xmin = mine ? L.x : 1 << 30;
+                int ymax = mine ? L.y : -1, xmax = mine ? L.x : -1;
+                int fmin = mine ? (int)f : 1 << 30, fmax = mine ? (int)f : -1;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
+                    xmin = min(xmin, __shfl_xor_sync(0xffffffffu, xmin, o));
+                    ymax = max(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
+                    xmax = max(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+                    fmin = min(fmin, __shfl_xor_sync(0xffffffffu, fmin, o));
+                    fmax = max(fmax, __shfl_xor_sync(0xffffffffu, fmax, o));
+                }
+                if (half == 0 && lane == 0) {
+                    int *q = bbx + 8 * (r >> 5);
+                    q[0] = ymin; q[1] = xmin; q[2] = ymax; q[3] = xmax; q[4] = fmin; q[5] = fmax;
+                }
+                tc::wg_sync(bar_id, TEAM);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    ymin = min(ymin, bbx[8 * q]); xmin = min(xmin, bbx[8 * q + 1]);
+                    ymax = max(ymax, bbx[8 * q + 2]); xmax = max(xmax, bbx[8 * q + 3]);
+                    fmin = min(fmin, bbx[8 * q + 4]); fmax = max(fmax, bbx[8 * q + 5]);
+                }
+                if (!a.vbm3d && ymax >= 0 && fmin == fmax) {
+                    y0 = ymin;
+                    x0 = xmin & ~3;
+                    rh = ymax + 8 - ymin;
+                    // whole 16-byte chunks, never past the padded row (ld is a multiple of 32)
+                    rw = min((xmax + 8 - x0 + 3) & ~3, a.ld - x0);
+                    region = rh * rw <= Shp::kRegion;
+                    frame = fmin;
+                }
+            }
+            // 1. gather (rows of foreign or partial groups are zero), one block per warp step
+            if (region) {
+                const long long fo = (long long)frame * a.frame_stride;
+                const int nv = rh * (rw >> 2);
+                for (int pass = WIENER ? 0 : 1; pass < 2; ++pass) {
+                    // pass 0: reference plane -> R; pass 1: source plane -> X
+                    const float *plane = (pass == 0 ? a.ref[p] : a.src[p]) + fo + (long long)y0 * a.ld + x0;
+                    unsigned char *dst = D + (pass == 0 ? Lay::kXBytes : 0);
+                    for (int v = t; v < nv; v += TEAM) {
+                        const int yy = v / (rw >> 2), c4 = v - yy * (rw >> 2);
+                        tc::cp_async16(Rg + yy * rw + 4 * c4, plane + (long long)yy * a.ld + 4 * c4);
+                    }
+                    tc::cp_async_wait_all();
+                    tc::wg_sync(bar_id, TEAM);
+#pragma unroll 4
+                    for (int i = half * NI; i < half * NI + NI; ++i) {
+                        const bool mi = __shfl_sync(0xffffffffu, mine, i);
+                        const int by = __shfl_sync(0xffffffffu, L.y, i) - y0, bx = __shfl_sync(0xffffffffu, L.x, i) - x0;
+                        float v0 = 0.f, v1 = 0.f;
+                        if (mi) {
+                            v0 = Rg[(by + ry) * rw + bx + cx];
+                            v1 = Rg[(by + ry + 4) * rw + bx + cx];
+                        }
+                        *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane, 128)) = v0;
+                        *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
+                    }
+                    tc::wg_sync(bar_id, TEAM);
+                }
+            } else {
                 const float *sp = L.src + (long long)L.y * a.ld + L.x;
                 const float *rp = L.ref + (long long)L.y * a.ld + L.x;
-                const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
-                const int b0 = r & ~31;
 #pragma unroll 4
                 for (int i = half * NI; i < half * NI + NI; ++i) {
                     const bool mi = __shfl_sync(0xffffffffu, mine, i);
@@ -320,21 +397,70 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
 #pragma unroll
                 for (int c = 0; c < NC; c += 4)
                     *reinterpret_cast<float4 *>(D + tc::sw128_offset(r, cb + c, 128)) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
-                if constexpr (SPLIT == 2) tc::wg_sync(bar_id, TEAM);
-                else __syncwarp();
+                // Region mode accumulates in 32-bit fixed point: integer shared-memory atomics are
+                // native, float ones are not.  The scale is a power of two chosen per tile so that
+                // 128 contributions of the largest magnitude stay below 2^30.
+                float cmax = 0.0f;
+                if (region && mine) {
+#pragma unroll
+                    for (int c = 0; c < NC; ++c) cmax = fmaxf(cmax, fabsf(v[c]));
+                    cmax *= numW;
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) cmax = fmaxf(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+                if ((t & 31) == 0) reinterpret_cast<float *>(bbx)[t >> 5] = cmax;
+                int *Ri = reinterpret_cast<int *>(Rg);
+                if (region)
+                    for (int e = t; e < rh * rw; e += TEAM) Ri[e] = 0;
+                tc::wg_sync(bar_id, TEAM);
+                float scale = 1073741824.0f;                 // 2^30
+                if (region) {
+#pragma unroll
+                    for (int q = 0; q < TEAM / 32; ++q) cmax = fmaxf(cmax, reinterpret_cast<const float *>(bbx)[q]);
+                    if (cmax > 1e-20f) {
+                        int ex;
+                        frexpf(1073741824.0f / (128.0f * cmax), &ex);   // 2^(ex-1) <= bound < 2^ex
+                        scale = ldexpf(1.0f, ex - 1);
+                    } else if (cmax > 0.0f) {
+                        scale = 1.0e30f;                         // contributions below 1e-20
+                    }
+                }
                 float *np = L.num + (long long)L.y * a.ld + L.x;
-                const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
-                const int b0 = r & ~31;
 #pragma unroll 4
                 for (int i = half * NI; i < half * NI + NI; ++i) {
                     const bool mi = __shfl_sync(0xffffffffu, mine, i);
-                    float *ni = reinterpret_cast<float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(np), i));
                     const float wi = __shfl_sync(0xffffffffu, numW, i);
-                    if (mi) {
-                        const float x0 = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane, 128));
-                        const float x1 = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128));
-                        atomicAdd(ni + (long long)ry * a.ld + cx, x0 * wi);
-                        atomicAdd(ni + (long long)(ry + 4) * a.ld + cx, x1 * wi);
+                    if (region) {
+                        const int by = __shfl_sync(0xffffffffu, L.y, i) - y0, bx = __shfl_sync(0xffffffffu, L.x, i) - x0;
+                        if (mi) {
+                            const float x0v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane, 128));
+                            const float x1v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128));
+                            atomicAdd(Ri + (by + ry) * rw + bx + cx, __float2int_rn(x0v * wi * scale));
+                            atomicAdd(Ri + (by + ry + 4) * rw + bx + cx, __float2int_rn(x1v * wi * scale));
+                        }
+                    } else {
+                        float *ni = reinterpret_cast<float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(np), i));
+                        if (mi) {
+                            const float x0v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane, 128));
+                            const float x1v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128));
+                            atomicAdd(ni + (long long)ry * a.ld + cx, x0v * wi);
+                            atomicAdd(ni + (long long)(ry + 4) * a.ld + cx, x1v * wi);
+                        }
+                    }
+                }
+                if (region) {
+                    // the region's sums, one vector atomic per 4 pixels (untouched ones skipped)
+                    tc::wg_sync(bar_id, TEAM);
+                    float *nbase = a.num[p] + (long long)frame * a.frame_stride + (long long)y0 * a.ld + x0;
+                    const int nv = rh * (rw >> 2);
+                    for (int e = t; e < nv; e += TEAM) {
+                        const int yy = e / (rw >> 2), c4 = e - yy * (rw >> 2);
+                        const int4 qi = *reinterpret_cast<const int4 *>(Ri + yy * rw + 4 * c4);
+                        if (qi.x != 0 || qi.y != 0 || qi.z != 0 || qi.w != 0) {
+                            const float inv = 1.0f / scale;
+                            const float4 q = make_float4((float)qi.x * inv, (float)qi.y * inv, (float)qi.z * inv, (float)qi.w * inv);
+                            atomicAdd(reinterpret_cast<float4 *>(nbase + (long long)yy * a.ld + 4 * c4), q);
+                        }
                     }
                 }
             }

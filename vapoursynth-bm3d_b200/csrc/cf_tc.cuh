@@ -156,6 +156,15 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             tc::mma_ss_tf32(tb + d0, tc::make_desc_sw128(sx + (s / 4) * 16 * 1024 + (s % 4) * 32, 1024),
                             tc::make_desc(sk + s * 256, 128, 2048), ID64, s > 0);
     };
+    // two independent 2-D products (source and reference) issued alternately
+    auto xy_ss2 = [&](uint32_t d0, uint32_t sx, uint32_t d1, uint32_t sy, uint32_t sk) {
+#pragma unroll 1
+        for (int s = 0; s < 8; ++s) {
+            const uint64_t bd = tc::make_desc(sk + s * 256, 128, 2048);
+            tc::mma_ss_tf32(tb + d0, tc::make_desc_sw128(sx + (s / 4) * 16 * 1024 + (s % 4) * 32, 1024), bd, ID64, s > 0);
+            tc::mma_ss_tf32(tb + d1, tc::make_desc_sw128(sy + (s / 4) * 16 * 1024 + (s % 4) * 32, 1024), bd, ID64, s > 0);
+        }
+    };
     // 2-D stage, A in tensor memory: D[d0, +64) = T[a0, +64) . K
     auto xy_ts = [&](uint32_t d0, uint32_t a0, uint32_t sk) {
 #pragma unroll 1
@@ -164,20 +173,22 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     };
     // z stage: rows of group w of D[d0, +nt) = Zstack . Bt_w (K range of group w), every other
     // output lane disabled; Bt swizzled [nt rows][128 k]
+    // The per-group chains are independent (disjoint output lanes), so consecutive products go
+    // to different groups: K step outer, group inner.
     auto z_stage = [&](uint32_t d0, uint32_t sz, int nt, uint32_t idesc) {
 #pragma unroll 1
-        for (int w = 0; w < GPT; ++w) {
-            uint32_t m[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int lo = G * w - 32 * q, hi = lo + G;      // enabled lanes of word q: [lo, hi)
-                const uint32_t en = (hi <= 0 || lo >= 32) ? 0u
-                                  : (G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lo < 0 ? 0 : lo)));
-                m[q] = ~en;
-            }
+        for (int s = 0; s < G / 8; ++s) {
+            const uint64_t ad = tc::make_desc(sz + s * 256, 128, (G / 4) * 128);
 #pragma unroll 1
-            for (int s = 0; s < G / 8; ++s) {
-                const uint64_t ad = tc::make_desc(sz + s * 256, 128, (G / 4) * 128);
+            for (int w = 0; w < GPT; ++w) {
+                uint32_t m[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int lo = G * w - 32 * q, hi = lo + G;      // enabled lanes of word q: [lo, hi)
+                    const uint32_t en = (hi <= 0 || lo >= 32) ? 0u
+                                      : (G == 32 ? 0xffffffffu : (((1u << G) - 1u) << (lo < 0 ? 0 : lo)));
+                    m[q] = ~en;
+                }
                 const uint32_t k0 = (uint32_t)(G * w + 8 * s);
                 const uint64_t bd = tc::make_desc_sw128(sD + (k0 / 32) * (nt / 8) * 1024 + ((k0 % 32) / 8) * 32, 1024);
                 tc::mma_ss_tf32_masked(tb + d0, ad, bd, idesc, s > 0, m[0], m[1], m[2], m[3]);
@@ -309,8 +320,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             publish();
             // 2. 2-D DCT
             if (t == 0) {
-                xy_ss(0, sD, sKf);
-                if constexpr (WIENER) xy_ss(64, sD + Lay::kXBytes, sKf);
+                if constexpr (WIENER) xy_ss2(0, sD, 64, sD + Lay::kXBytes, sKf);
+                else xy_ss(0, sD, sKf);
                 tc::mma_commit(mb);
             }
             if (!wait_mma()) { failed = true; break; }

@@ -174,6 +174,15 @@ BM3D_API int bm3d_debug_matches(bm3d_filter *filter, int k, int *counts, int *zs
  * of stages written (0 when nothing was recorded). */
 BM3D_API int bm3d_set_profiling(bm3d_filter *filter, int enable);
 BM3D_API int bm3d_debug_stage_times(bm3d_filter *filter, double *ms, int capacity);
+/* FP64 GPU oracle: frame k of the last bm3d_get_frames call of a Basic or Final filter recomputed
+ * in double precision from the filter's own match lists -- 3-D DCTs, hard threshold or Wiener
+ * shrinkage, aggregation and normalisation (source/BM3D_Basic.cpp:72-148,
+ * source/BM3D_Final.cpp:50-127, source/BM3D_Base.cpp:348-351), thresholds and variances in double.
+ * Writes the processed planes of the internal float domain (the filter's output before any
+ * output-format conversion) as doubles to HOST memory, planes[p * plane_stride + y * width + x].
+ * Returns 0, or -1 (V-BM3D filter, no such frame, or block/group size beyond its shared memory).
+ * An inspection tool for the error of the FP32 and tf32 forms; it allocates device memory. */
+BM3D_API int bm3d_debug_reference_fp64(bm3d_filter *filter, int k, double *planes, int64_t plane_stride);
 /* Number of kernels this library has launched since it was loaded (all filters). */
 BM3D_API int64_t bm3d_debug_launch_count(void);
 /* Number of reference blocks that took the exact tie-resolution path in the last call. */

@@ -297,6 +297,17 @@ class FilterNode(VideoNode):
         return (counts[:nb], z[:nb * g].reshape(nb, g), y[:nb * g].reshape(nb, g), x[:nb * g].reshape(nb, g),
                 keys[:nb * g].reshape(nb, g))
 
+    def reference_fp64(self, k=0):
+        """FP64 GPU oracle of output frame k of the last computed batch (Basic / Final): float64
+        [planes][H][W] in the filter's internal float domain (planes not processed are zero)."""
+        L = capi.lib()
+        info = self.info
+        out = np.zeros((3, info.height, info.width), np.float64)
+        rc = L.bm3d_debug_reference_fp64(self._h, k, out.ctypes.data_as(C.POINTER(C.c_double)), info.height * info.width)
+        if rc != 0:
+            raise Error("no FP64 reference for this filter / frame")
+        return out
+
     def slow_blocks(self):
         return int(capi.lib().bm3d_debug_slow_blocks(self._h))
 

@@ -146,6 +146,15 @@ struct ConvProgram {
 };
 
 // finalize: out = num / box_B(wmap) for processed planes of a batch of frames.
+// FP64 oracle outputs and constants (inspection only)
+struct F64Args {
+    double *num[3];
+    double *den[3];          // per-pixel denominator (not the per-origin weight map)
+    double sigma[3];         // sigma / 255 * matrix norm, per plane
+    double lambda;
+    long long out_stride;    // doubles between rows of num / den
+};
+
 struct FinalizeArgs {
     const float *num[3];
     const float *wmap[3];

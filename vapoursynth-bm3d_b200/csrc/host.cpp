@@ -578,6 +578,7 @@ public:
     virtual int run(int n, int count, const bm3d_frame *const *src, const bm3d_frame *const *ref,
                     bm3d_frame *const *dst, bool sync) = 0;
     virtual int matches(int, int *, int *, int *, int *, float *, int) { return -1; }
+    virtual int reference_fp64(int, double *, long long) { return -1; }
     // called after the filter's stream was synchronised (device-side error flags)
     virtual void synced() {}
     int nplanes() const { return vi.color_family == BM3D_GRAY ? 1 : 3; }
@@ -695,6 +696,7 @@ public:
     bool wiener = false;
     bool vbm3d = false;
     bool tc = false;            // precision form: tensor-core transforms (argument "precision")
+    double plane_sigma[3] = {0, 0, 0};
     Params para, para_default;
     int matrix = MAT_UNSPEC;
     int process[3] = {1, 1, 1};
@@ -838,6 +840,7 @@ public:
         double norm[3];
         matrix_norms(matrix, norm);
         normY = norm[0];
+        for (int c = 0; c < 3; ++c) plane_sigma[c] = para.sigma[c] / double(255) * norm[c];
         para.thMSE *= normY;
         for (int c = 0; c < 3; ++c)
             if (process[c]) tables[c] = plane_tables(wiener, para.sigma[c] / double(255) * norm[c], para.G, para.B, para.lambda);
@@ -1073,6 +1076,48 @@ public:
             a.skip_full = 0;
             CU(launch_cf_generic(a, 4, (int)(gwarps / 4), stream));
         }
+    }
+
+    // FP64 oracle of frame k of the last batch (BM3D filters): planes [p][H][W] to host memory
+    int reference_fp64(int k, double *out, long long plane_stride) override
+    {
+        if (vbm3d || k < 0 || k >= last_count) return -1;
+        if (para.G > 64 || para.B > 64 || cf_fp64_smem(para.B, para.G) > 200 * 1024) return -1;
+        const long long bpf = (long long)sy.size() * sx.size();
+        CFArgs a{};
+        DevBuf *refws = rdef ? ws_ref : ws_src;
+        F64Args f{};
+        DevBuf nd[3], dd[3];
+        const size_t pl = (size_t)H * W;
+        for (int p = 0; p < 3; ++p) {
+            a.process[p] = process[p] && p < nplanes();
+            a.src[p] = ws_src[p].as<float>() + k * fs;
+            a.ref[p] = (wiener ? refws[p].as<float>() : ws_src[p].as<float>()) + k * fs;
+            f.sigma[p] = plane_sigma[p];
+            if (!a.process[p]) continue;
+            f.num[p] = static_cast<double *>(nd[p].get(sizeof(double) * pl));
+            f.den[p] = static_cast<double *>(dd[p].get(sizeof(double) * pl));
+            CU(cudaMemsetAsync(f.num[p], 0, sizeof(double) * pl, stream));
+            CU(cudaMemsetAsync(f.den[p], 0, sizeof(double) * pl, stream));
+        }
+        f.lambda = para.lambda;
+        f.out_stride = W;
+        a.frame_stride = fs;
+        a.ld = ld;
+        a.H = H;
+        a.W = W;
+        a.B = para.B;
+        a.G = para.G;
+        a.wiener = wiener;
+        a.pos = m_pos.as<uint32_t>() + (size_t)k * bpf * para.G;
+        a.count = m_n.as<int>() + (size_t)k * bpf;
+        a.ngroups = bpf;
+        a.blocks_per_frame = bpf;
+        CU(launch_cf_fp64(a, f, stream));
+        CU(cudaStreamSynchronize(stream));
+        for (int p = 0; p < 3; ++p)
+            if (a.process[p]) CU(cudaMemcpy(out + p * plane_stride, f.num[p], sizeof(double) * pl, cudaMemcpyDeviceToHost));
+        return 0;
     }
 
     int matches(int k, int *counts, int *zs, int *ys, int *xs, float *keys, int cap) override
@@ -1810,6 +1855,18 @@ BM3D_API int bm3d_debug_stage_times(bm3d_filter *h, double *ms, int capacity)
         return 0;
     });
     return n;
+}
+
+BM3D_API int bm3d_debug_reference_fp64(bm3d_filter *h, int k, double *planes, int64_t plane_stride)
+{
+    if (!h || !planes) return -1;
+    std::lock_guard<std::mutex> lk(h->mu);
+    int r = -1;
+    guarded([&]() {
+        r = h->f->reference_fp64(k, planes, (long long)plane_stride);
+        return 0;
+    });
+    return r;
 }
 
 BM3D_API int64_t bm3d_debug_launch_count(void) { return (int64_t)launch_count(); }

@@ -7,6 +7,7 @@
 #include "vbm.cuh"
 #include "cf.cuh"
 #include "cf_tc.cuh"
+#include "fp64.cuh"
 #include "convert.cuh"
 #include "launch.h"
 #include "params.h"
@@ -165,6 +166,26 @@ cudaError_t launch_cf_tc(const CFArgs &a, const void *tables, int *status, cudaS
     case 16: return w ? launch_cf_tc_t<16, true>(a, tables, status, s) : launch_cf_tc_t<16, false>(a, tables, status, s);
     default: return w ? launch_cf_tc_t<32, true>(a, tables, status, s) : launch_cf_tc_t<32, false>(a, tables, status, s);
     }
+}
+
+// ---- FP64 oracle (inspection) --------------------------------------------------------------------
+
+size_t cf_fp64_smem(int B, int G) { return sizeof(double) * ((size_t)2 * G * B * B + 64 * 64); }
+
+cudaError_t launch_cf_fp64(const CFArgs &a, const F64Args &f, cudaStream_t s)
+{
+    const size_t smem = cf_fp64_smem(a.B, a.G);
+    cudaError_t e;
+    // always raised: the kernel's static shared memory comes on top of the dynamic part
+    if ((e = cudaFuncSetAttribute(cf_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+        return e;
+    COUNT_LAUNCH();
+    cf_fp64_kernel<<<(unsigned)a.ngroups, 64, smem, s>>>(a, f);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    dim3 grid((a.W + 127) / 128, a.H, 3);
+    COUNT_LAUNCH();
+    finalize_fp64_kernel<<<grid, 128, 0, s>>>(f, a.W, a.H, 1, a.process[0], a.process[1], a.process[2]);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_cf_generic(const CFArgs &a, int warps, int grid, cudaStream_t s)

@@ -40,6 +40,12 @@ int cf_tc_supported(int B, int G);
 void cf_tc_tables(int G, std::vector<unsigned char> &img);
 cudaError_t launch_cf_tc(const CFArgs &a, const void *tables, int *status, cudaStream_t s);
 
+// FP64 oracle of the collaborative filter, aggregation and normalisation for the groups of one
+// frame (a.ngroups = a.blocks_per_frame); writes num / den into f.num.  Inspection only.
+struct F64Args;
+size_t cf_fp64_smem(int B, int G);
+cudaError_t launch_cf_fp64(const CFArgs &a, const F64Args &f, cudaStream_t s);
+
 // Number of kernels launched by this library since load.
 unsigned long long launch_count();
 

@@ -22,6 +22,7 @@
 
 #include "select.cuh"
 #include "args.h"
+#include "tc.cuh"
 
 namespace bm3d {
 
@@ -256,11 +257,14 @@ __global__ void __launch_bounds__(256) bm_full_kernel(BMArgs a)
     const int ww = wx1 - wx0;
     const int wp = a.win_pitch;
 
+    // window rows, one warp per row, asynchronous 4-byte copies (no register round trip)
     float *win = smem;
-    for (int idx = threadIdx.x; idx < (wy1 - wy0) * ww; idx += blockDim.x) {
-        const int yy = idx / ww, xx = idx - yy * ww;
-        win[yy * wp + xx] = __ldg(plane + (long long)(wy0 + yy) * a.ld + wx0 + xx);
+    for (int yy = warp; yy < wy1 - wy0; yy += (int)(blockDim.x >> 5)) {
+        const float *src = plane + (long long)(wy0 + yy) * a.ld + wx0;
+        float *dst = win + yy * wp;
+        for (int xx = lane; xx < ww; xx += 32) tc::cp_async4(dst + xx, src + xx);
     }
+    tc::cp_async_wait_all();
     __syncthreads();
     if (bx >= a.nbx) return;
 

@@ -75,6 +75,11 @@ struct TcShape {
     static constexpr int kRegion = 3072;                  // floats of the staged image region
     static constexpr int kExtra = kPart + kRegion * 4 + 128;   // + [4 quarters][8] ints of bounds
     static constexpr int kSmem = (kData + kExtra) * kWG + TcLayout<G>::kTableBytes;
+    // With two teams, tensor memory has room for the z-stage matrix stacks (G columns each): the
+    // z products then read A from tensor memory and only B from shared memory.
+    static constexpr bool kZInTmem = kWG == 2 && G >= 16;
+    static constexpr int kTmemCols = kWG == 4 ? 512 : (kZInTmem ? 512 : 256);
+    static constexpr int kZCol = 128 * kWG;              // first column of the stacks
 };
 
 // byte offset of element (row, k) of a K-major operand with `kdim` columns
@@ -120,13 +125,33 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
 
     for (int i = threadIdx.x; i < Lay::kTableBytes / 16; i += blockDim.x)
         reinterpret_cast<float4 *>(tab)[i] = tables[i];
-    if (warp == 0) tc::tmem_alloc(&tslot, 128 * NWG);
+    if (warp == 0) tc::tmem_alloc(&tslot, Shp::kTmemCols);
     if (t == 0) tc::mbar_init(&mbar[wg], 1);
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tm = tslot;
+    if constexpr (Shp::kZInTmem) {
+        // row threadIdx.x of both stacks -> tensor-memory lane threadIdx.x (warps 0..3)
+        if (threadIdx.x < 128) {
+            const uint32_t lr = (uint32_t)(32 * (threadIdx.x >> 5)) << 16;
+#pragma unroll
+            for (int m = 0; m < 2; ++m)
+#pragma unroll
+                for (int k0 = 0; k0 < G; k0 += 16) {
+                    float v[16];
+#pragma unroll
+                    for (int e = 0; e < 16; ++e)
+                        v[e] = *reinterpret_cast<const float *>(tab + (m ? Lay::kZi : Lay::kZf) + tc_kmajor(threadIdx.x, k0 + e, G));
+                    tc::tmem_st16(tm + lr + Shp::kZCol + m * G + k0, v);
+                }
+            tc::tmem_wait_st();
+        }
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+    }
     const uint32_t tb = tm + 128 * wg;               // this warpgroup's columns
     const uint32_t lrow = (uint32_t)(32 * (warp & 3)) << 16;
     const uint32_t sZf = tc::smem_u32(tab + Lay::kZf), sZi = tc::smem_u32(tab + Lay::kZi);
@@ -191,7 +216,11 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 }
                 const uint32_t k0 = (uint32_t)(G * w + 8 * s);
                 const uint64_t bd = tc::make_desc_sw128(sD + (k0 / 32) * (nt / 8) * 1024 + ((k0 % 32) / 8) * 32, 1024);
-                tc::mma_ss_tf32_masked(tb + d0, ad, bd, idesc, s > 0, m[0], m[1], m[2], m[3]);
+                if constexpr (Shp::kZInTmem)
+                    tc::mma_ts_tf32_masked(tb + d0, tm + Shp::kZCol + (sz == sZi ? G : 0) + 8 * s, bd, idesc, s > 0,
+                                           m[0], m[1], m[2], m[3]);
+                else
+                    tc::mma_ss_tf32_masked(tb + d0, ad, bd, idesc, s > 0, m[0], m[1], m[2], m[3]);
             }
         }
     };
@@ -485,7 +514,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (warp == 0) tc::tmem_free(tm, 128 * NWG);
+    if (warp == 0) tc::tmem_free(tm, Shp::kTmemCols);
 }
 
 }  // namespace bm3d

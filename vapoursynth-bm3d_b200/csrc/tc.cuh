@@ -134,6 +134,16 @@ __device__ __forceinline__ void mma_ss_tf32_masked(uint32_t d_tmem, uint64_t a_d
                    "r"(m0), "r"(m1), "r"(m2), "r"(m3));
 }
 
+// D[tmem] (+)= A[tmem] * B[smem] with masked output lanes (see mma_ss_tf32_masked).
+__device__ __forceinline__ void mma_ts_tf32_masked(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
+                                                   bool accumulate, uint32_t m0, uint32_t m1, uint32_t m2, uint32_t m3)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+                 ::"r"(d_tmem), "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"((uint32_t)accumulate),
+                   "r"(m0), "r"(m1), "r"(m2), "r"(m3));
+}
+
 // D[tmem] (+)= A[tmem] * B[smem]; issued by one thread.  A occupies the same lanes as D, K columns.
 __device__ __forceinline__ void mma_ts_tf32(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc, bool accumulate)
 {

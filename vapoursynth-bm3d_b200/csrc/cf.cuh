@@ -401,6 +401,287 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
     }
 }
 
+// The warp's 32 blocks (lane i's block at sp of lane i) into rows i of S (pitch kTP), one block per
+// step with lane = (row, column) of the block: each load instruction touches one block's 4 rows
+// instead of 32 blocks, which is what the memory system can serve.  Then every lane reads its own
+// row back into registers.
+__device__ __forceinline__ void gather_blocks8(float (&blk)[64], float *S, const float *sp, int ld, int lane)
+{
+    const int ry = lane >> 3, cx = lane & 7;
+#pragma unroll 4
+    for (int i = 0; i < 32; ++i) {
+        const float *q = reinterpret_cast<const float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(sp), i));
+        S[i * kTP + lane] = __ldg(q + (long long)ry * ld + cx);
+        S[i * kTP + 32 + lane] = __ldg(q + (long long)(ry + 4) * ld + cx);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int e = 0; e < 64; ++e) blk[e] = S[lane * kTP + e];
+    __syncwarp();
+}
+
+// The run kernel, for the Final estimate over all groups of a BM3D frame: a run of kCfRunGroups
+// consecutive groups (consecutive reference blocks of one row) per CTA, one warp per G-group slot.  The blocks a run adds lie in one box of the
+// image (the search windows of its reference blocks); in region mode the run adds them into that
+// box in shared memory, in 64-bit fixed point (native integer atomics: shared-memory float
+// atomics are emulated), and flushes the box to the numerator plane once per plane with one
+// vector atomic per 4 pixels.  Flushing per run rather than per few groups matters: global
+// atomics on pixels that many neighbouring runs cover serialise at the L2.
+// Eight warps per CTA and one CTA per SM: the Final's two transpose buffers per warp and the box
+// fill the shared memory.  Measured on B200 for the Basic estimate (fewer, lighter overlaps) and
+// for the partial groups of the precision form (few active warps per run), the per-lane kernel
+// above is faster, so those keep it.
+constexpr int kCfWarps = 8;
+constexpr int kCfRunGroups = 32;
+constexpr int kCfCells = 7168;                 // int64 cells of the box (57 KB)
+constexpr float kCfFix = 4294967296.0f;        // 2^32: fixed-point scale of the box
+constexpr float kCfUnfix = 2.3283064365386963e-10f;   // 2^-32
+// Terms at or above 2^19 go to the plane directly: a pixel takes at most 32 groups x 64 block
+// positions = 2^11 terms per run, so the box sums stay below 2^62 in fixed point.
+constexpr float kCfFixMax = 524288.0f;
+
+template <int G, bool WIENER>
+__global__ void __launch_bounds__(kCfWarps * 32, 1) cf_run_kernel(CFArgs a)
+{
+    constexpr int GPW = 32 / G;
+    constexpr int C = 64 / G;
+    constexpr int TPG = kCfWarps * GPW;                         // groups per pass of the warps
+    constexpr int RUN = kCfRunGroups / TPG > 0 ? kCfRunGroups / TPG : 1;   // passes per run
+    extern __shared__ float smem[];
+    const int lane = (int)lane_id();
+    const int warp = threadIdx.x >> 5;
+    const int sub = lane / G;
+    const int z = lane - sub * G;
+    float *T = smem + warp * (WIENER ? 2 : 1) * 32 * kTP;
+    float *T2 = T + 32 * kTP;
+    unsigned long long *Rq = reinterpret_cast<unsigned long long *>(smem + kCfWarps * (WIENER ? 2 : 1) * 32 * kTP);
+    int *rb = reinterpret_cast<int *>(Rq + kCfCells);            // [warp][8] bounds
+    for (int e = threadIdx.x; e < kCfCells; e += blockDim.x) Rq[e] = 0ull;
+    __syncthreads();
+    const int ry = lane >> 3, cx = lane & 7;
+
+    for (long long run = blockIdx.x; run * RUN * TPG < a.ngroups; run += gridDim.x) {
+        // bounds of the blocks the run adds
+        int y0 = 0, x0 = 0, rh = 0, rw = 0, frame = 0;
+        bool region = false;
+        if (!a.skip_full && !a.vbm3d) {
+            int v[6] = {1 << 30, 1 << 30, -1, -1, 1 << 30, -1};
+            for (int t = 0; t < RUN; ++t) {
+                const long long grp = ((run * RUN + t) * kCfWarps + warp) * GPW + sub;
+                if (grp >= a.ngroups) continue;
+                const int n = min(a.count[grp], G);
+                if (z >= n) continue;
+                const uint32_t pk = a.pos[grp * G + z];
+                const int py = unpack_y(pk), px = unpack_x(pk), f = (int)(grp / a.blocks_per_frame);
+                v[0] = min(v[0], py); v[1] = min(v[1], px); v[2] = max(v[2], py); v[3] = max(v[3], px);
+                v[4] = min(v[4], f); v[5] = max(v[5], f);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                v[0] = min(v[0], __shfl_xor_sync(0xffffffffu, v[0], o));
+                v[1] = min(v[1], __shfl_xor_sync(0xffffffffu, v[1], o));
+                v[2] = max(v[2], __shfl_xor_sync(0xffffffffu, v[2], o));
+                v[3] = max(v[3], __shfl_xor_sync(0xffffffffu, v[3], o));
+                v[4] = min(v[4], __shfl_xor_sync(0xffffffffu, v[4], o));
+                v[5] = max(v[5], __shfl_xor_sync(0xffffffffu, v[5], o));
+            }
+            if (lane == 0)
+                for (int k = 0; k < 6; ++k) rb[warp * 8 + k] = v[k];
+            __syncthreads();
+            for (int w = 0; w < kCfWarps; ++w) {
+                v[0] = min(v[0], rb[w * 8]); v[1] = min(v[1], rb[w * 8 + 1]);
+                v[2] = max(v[2], rb[w * 8 + 2]); v[3] = max(v[3], rb[w * 8 + 3]);
+                v[4] = min(v[4], rb[w * 8 + 4]); v[5] = max(v[5], rb[w * 8 + 5]);
+            }
+            __syncthreads();
+            if (v[2] >= 0 && v[4] == v[5]) {
+                y0 = v[0];
+                x0 = v[1] & ~3;
+                rh = v[2] + 8 - v[0];
+                rw = min((v[3] + 8 - x0 + 3) & ~3, a.ld - x0);    // whole 16-byte chunks within the row
+                region = rh * rw <= kCfCells;
+                frame = v[4];
+            }
+        }
+        for (int p = 0; p < 3; ++p) {
+            if (!a.process[p]) continue;
+            for (int t = 0; t < RUN; ++t) {
+                const long long grp = ((run * RUN + t) * kCfWarps + warp) * GPW + sub;
+                const bool inrange = grp < a.ngroups;
+                const long long g0 = inrange ? grp : 0;
+                const int n = min(a.count[g0], G);
+                // skip_full: full groups were filtered by the tensor-core kernel; only partial ones here
+                const bool taken = a.skip_full && n == G;
+                const bool skipw = __all_sync(0xffffffffu, taken || !inrange);
+                const bool active = inrange && z < n && !taken;
+                const bool full = __all_sync(0xffffffffu, n == G);
+                const uint32_t pk = a.pos[g0 * G + min(z, n - 1)];
+                const GroupLoc L = locate(a, p, g0, pk);
+                float blk[64];
+                float denW = 0.0f;
+                if (!skipw) {
+                if constexpr (WIENER) {
+                    gather_blocks8(blk, T2, L.ref + (long long)L.y * a.ld + L.x, a.ld, lane);
+                    fwd2d8(blk);
+    #pragma unroll
+                    for (int e = 0; e < 64; ++e) T2[lane * kTP + e] = blk[e];
+                    __syncwarp();
+                    const float sg = a.wsig2[p][n - 1];
+                    if (full) {
+    #pragma unroll 1
+                        for (int q = 0; q < C; ++q) {
+                            float *Wc = T2 + sub * G * kTP + z + q * G;
+                            float col[G], R[G];
+    #pragma unroll
+                            for (int zz = 0; zz < G; ++zz) col[zz] = Wc[zz * kTP];
+                            fdct_reg<G>(col, R);
+    #pragma unroll
+                            for (int zz = 0; zz < G; ++zz) {
+                                const float r2 = __fmul_rn(R[zz], R[zz]);
+                                Wc[zz * kTP] = __fdiv_rn(r2, __fadd_rn(r2, sg));
+                            }
+                        }
+                    } else {
+                        const float *fwd = n == G ? nullptr : dtab_for(a, n, false);
+    #pragma unroll 1
+                        for (int q = 0; q < C; ++q) wiener_any<G>(T2 + sub * G * kTP + z + q * G, sg, n, fwd);
+                    }
+                    __syncwarp();
+                }
+                gather_blocks8(blk, T, L.src + (long long)L.y * a.ld + L.x, a.ld, lane);
+                fwd2d8(blk);
+    #pragma unroll
+                for (int e = 0; e < 64; ++e) T[lane * kTP + e] = blk[e];
+                __syncwarp();
+                int kept = 0;
+                float l2 = 0.0f;
+                if (full) {
+    #pragma unroll 1
+                    for (int q = 0; q < C; ++q) {
+                        const int c = z + q * G;
+                        float *Tc = T + sub * G * kTP + c;
+                        float col[G], X[G];
+    #pragma unroll
+                        for (int zz = 0; zz < G; ++zz) col[zz] = Tc[zz * kTP];
+                        fdct_reg<G>(col, X);
+                        if constexpr (!WIENER) {
+                            const int fxy = ((c & 7) == 0) + ((c >> 3) == 0);
+                            const float t0 = a.thr4[p][G - 1][fxy + 1];
+                            const float t1 = a.thr4[p][G - 1][fxy];
+    #pragma unroll
+                            for (int zz = 0; zz < G; ++zz) {
+                                const float th = zz == 0 ? t0 : t1;
+                                const bool keep = fabsf(X[zz]) > th;
+                                kept += keep;
+                                X[zz] = keep ? X[zz] : 0.0f;
+                            }
+                        } else {
+                            const float *Wc = T2 + sub * G * kTP + c;
+    #pragma unroll
+                            for (int zz = 0; zz < G; ++zz) {
+                                const float w = Wc[zz * kTP];
+                                X[zz] = __fmul_rn(X[zz], w);
+                                l2 = __fadd_rn(l2, __fmul_rn(w, w));
+                            }
+                        }
+                        idct_reg<G>(X, col);
+    #pragma unroll
+                        for (int zz = 0; zz < G; ++zz) Tc[zz * kTP] = col[zz];
+                    }
+                } else {
+                    const float *fwd = dtab_for(a, n, false);
+                    const float *inv = dtab_for(a, n, true);
+    #pragma unroll 1
+                    for (int q = 0; q < C; ++q) {
+                        const int c = z + q * G;
+                        const int fxy = ((c & 7) == 0) + ((c >> 3) == 0);
+                        const float t0 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy + 1];
+                        const float t1 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy];
+                        const float r = zstage_any<G, WIENER>(T + sub * G * kTP + c, WIENER ? T2 + sub * G * kTP + c : nullptr,
+                                                              t0, t1, n, n == G ? nullptr : fwd, n == G ? nullptr : inv);
+                        if constexpr (!WIENER) kept += (int)r;
+                        else l2 = __fadd_rn(l2, r);
+                    }
+                }
+    #pragma unroll
+                for (int o = G / 2; o > 0; o >>= 1) {
+                    if constexpr (!WIENER) kept += __shfl_xor_sync(0xffffffffu, kept, o);
+                    else l2 = __fadd_rn(l2, __shfl_xor_sync(0xffffffffu, l2, o));
+                }
+                __syncwarp();
+    #pragma unroll
+                for (int e = 0; e < 64; ++e) blk[e] = T[lane * kTP + e];
+                __syncwarp();
+                inv2d8(blk);
+                if constexpr (!WIENER) {
+                    denW = kept < 1 ? 1.0f : __fdiv_rn(1.0f, (float)kept);
+                } else {
+                    const float eps = 1.1920928955078125e-07f;
+                    denW = __fdiv_rn(1.0f, l2 > eps ? l2 : eps);
+                }
+                const float numW = __fdiv_rn(denW, a.amp[n - 1]);
+    #pragma unroll
+                for (int e = 0; e < 64; ++e) T[lane * kTP + e] = __fmul_rn(blk[e], numW);
+                __syncwarp();
+                }   // !skipw
+                // aggregation one block per step (lane = pixel row / column), as for the gathers
+                if (!skipw) {
+                    if (region) {
+#pragma unroll 4
+                        for (int i = 0; i < 32; ++i) {
+                            const bool ai = __shfl_sync(0xffffffffu, active, i);
+                            const uint32_t pi = __shfl_sync(0xffffffffu, pk, i);
+                            if (ai) {
+                                const int by = unpack_y(pi) - y0, bx = unpack_x(pi) - x0;
+#pragma unroll
+                                for (int h = 0; h < 2; ++h) {
+                                    const float val = T[i * kTP + 32 * h + lane];
+                                    const int yy = by + ry + 4 * h, xx = bx + cx;
+                                    if (fabsf(val) < kCfFixMax)
+                                        atomicAdd(Rq + yy * rw + xx, (unsigned long long)__float2ll_rn(val * kCfFix));
+                                    else
+                                        atomicAdd(a.num[p] + (long long)frame * a.frame_stride + (long long)(y0 + yy) * a.ld + x0 + xx, val);
+                                }
+                            }
+                        }
+                    } else {
+                        float *np = L.num + (long long)L.y * a.ld + L.x;
+#pragma unroll 4
+                        for (int i = 0; i < 32; ++i) {
+                            const bool ai = __shfl_sync(0xffffffffu, active, i);
+                            float *q = reinterpret_cast<float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(np), i));
+                            if (ai) {
+                                atomicAdd(q + (long long)ry * a.ld + cx, T[i * kTP + lane]);
+                                atomicAdd(q + (long long)(ry + 4) * a.ld + cx, T[i * kTP + 32 + lane]);
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+                if (active) atomicAdd(L.wmap + (long long)L.y * a.ld + L.x, denW);
+            }
+            if (region) {
+                // the box to the numerator plane, then cleared for the next plane / run
+                __syncthreads();
+                float *nbase = a.num[p] + (long long)frame * a.frame_stride + (long long)y0 * a.ld + x0;
+                const int nv = rh * (rw >> 2);
+                for (int e = threadIdx.x; e < nv; e += blockDim.x) {
+                    const int yy = e / (rw >> 2), c4 = e - yy * (rw >> 2);
+                    unsigned long long *cell = Rq + yy * rw + 4 * c4;
+                    const long long q0 = (long long)cell[0], q1 = (long long)cell[1], q2 = (long long)cell[2], q3 = (long long)cell[3];
+                    if (q0 | q1 | q2 | q3) {
+                        atomicAdd(reinterpret_cast<float4 *>(nbase + (long long)yy * a.ld + 4 * c4),
+                                  make_float4(__ll2float_rn(q0) * kCfUnfix, __ll2float_rn(q1) * kCfUnfix,
+                                              __ll2float_rn(q2) * kCfUnfix, __ll2float_rn(q3) * kCfUnfix));
+                        cell[0] = cell[1] = cell[2] = cell[3] = 0ull;
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+}
+
 // ---- generic path: any B <= 64, any n <= 256; one warp per group, data in global scratch ----
 
 __device__ void dct3d_warp(float *g, int n, int B, bool inverse, const CFArgs &a, float *tmp)

@@ -72,14 +72,20 @@ struct TcShape {
     static constexpr int kTeam = 128 * kSplit;          // threads per team
     static constexpr int kData = TcLayout<G>::kXBytes * (WIENER ? 2 : 1);
     static constexpr int kPart = kSplit == 2 ? kTeam * 4 : 0; // per-row partial sums of the two halves
-    static constexpr int kRegion = 3072;                  // floats of the staged image region
-    static constexpr int kExtra = kPart + kRegion * 4 + 128;   // + [4 quarters][8] ints of bounds
-    static constexpr int kSmem = (kData + kExtra) * kWG + TcLayout<G>::kTableBytes;
     // With two teams, tensor memory has room for the z-stage matrix stacks (G columns each): the
-    // z products then read A from tensor memory and only B from shared memory.
+    // z products then read A from tensor memory and only B from shared memory, and the stacks
+    // need no shared-memory copy.
     static constexpr bool kZInTmem = kWG == 2 && G >= 16;
     static constexpr int kTmemCols = kWG == 4 ? 512 : (kZInTmem ? 512 : 256);
     static constexpr int kZCol = 128 * kWG;              // first column of the stacks
+    static constexpr int kTabOff = kZInTmem ? TcLayout<G>::kKf : 0;   // first table byte kept in shared memory
+    // Image boxes of the region mode: Final with the stacks in tensor memory keeps a source box,
+    // a reference box and the aggregation box, so that the next plane's boxes load while this
+    // plane is filtered; otherwise one box serves the gathers and the aggregation in turn.
+    static constexpr int kBoxes = WIENER && kZInTmem ? 3 : 1;
+    static constexpr int kRegion = kBoxes == 3 ? 2688 : 3072;   // floats per box
+    static constexpr int kExtra = kPart + kRegion * 4 * kBoxes + 128;   // + [4 quarters][8] ints of bounds
+    static constexpr int kSmem = (kData + kExtra) * kWG + TcLayout<G>::kTableBytes - kTabOff;
 };
 
 // byte offset of element (row, k) of a K-major operand with `kdim` columns
@@ -119,12 +125,17 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     unsigned char *D = tsm + Shp::kData * wg;        // X | R, then Yt, then St
     unsigned char *extra = tsm + Shp::kData * NWG + Shp::kExtra * wg;
     float *part = reinterpret_cast<float *>(extra);
-    float *Rg = reinterpret_cast<float *>(extra + Shp::kPart);         // staged region / accumulator
-    int *bbx = reinterpret_cast<int *>(extra + Shp::kPart + Shp::kRegion * 4);   // [4 quarters][8]
-    unsigned char *tab = tsm + (Shp::kData + Shp::kExtra) * NWG;
+    float *Rg = reinterpret_cast<float *>(extra + Shp::kPart);         // aggregation box
+    float *Bs = Shp::kBoxes == 3 ? Rg + Shp::kRegion : Rg;              // source box
+    float *Br = Shp::kBoxes == 3 ? Rg + 2 * Shp::kRegion : Rg;          // reference box
+    int *bbx = reinterpret_cast<int *>(extra + Shp::kPart + Shp::kRegion * 4 * Shp::kBoxes);   // [4 quarters][8]
+    // table byte b lives at tab + b (b >= kTabOff)
+    unsigned char *tab = tsm + (Shp::kData + Shp::kExtra) * NWG - Shp::kTabOff;
 
-    for (int i = threadIdx.x; i < Lay::kTableBytes / 16; i += blockDim.x)
-        reinterpret_cast<float4 *>(tab)[i] = tables[i];
+    for (int i = threadIdx.x; i < (Lay::kTableBytes - Shp::kTabOff) / 16; i += blockDim.x)
+        reinterpret_cast<float4 *>(tab + Shp::kTabOff)[i] = tables[Shp::kTabOff / 16 + i];
+    if constexpr (Shp::kBoxes == 3)
+        for (int i = t; i < Shp::kRegion; i += TEAM) Rg[i] = 0.0f;   // the aggregation box starts (and stays) zero
     if (warp == 0) tc::tmem_alloc(&tslot, Shp::kTmemCols);
     if (t == 0) tc::mbar_init(&mbar[wg], 1);
     tc::fence_proxy_async_smem();
@@ -143,7 +154,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     float v[16];
 #pragma unroll
                     for (int e = 0; e < 16; ++e)
-                        v[e] = *reinterpret_cast<const float *>(tab + (m ? Lay::kZi : Lay::kZf) + tc_kmajor(threadIdx.x, k0 + e, G));
+                        v[e] = __ldg(reinterpret_cast<const float *>(tables) + ((m ? Lay::kZi : Lay::kZf) + tc_kmajor(threadIdx.x, k0 + e, G)) / 4);
                     tc::tmem_st16(tm + lr + Shp::kZCol + m * G + k0, v);
                 }
             tc::tmem_wait_st();
@@ -154,7 +165,9 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     }
     const uint32_t tb = tm + 128 * wg;               // this warpgroup's columns
     const uint32_t lrow = (uint32_t)(32 * (warp & 3)) << 16;
-    const uint32_t sZf = tc::smem_u32(tab + Lay::kZf), sZi = tc::smem_u32(tab + Lay::kZi);
+    // (with the stacks in tensor memory, sZf / sZi only tell the two z products apart)
+    const uint32_t sZf = Shp::kZInTmem ? 0u : tc::smem_u32(tab + Lay::kZf);
+    const uint32_t sZi = Shp::kZInTmem ? 1u : tc::smem_u32(tab + Lay::kZi);
     const uint32_t sKf = tc::smem_u32(tab + Lay::kKf), sKi = tc::smem_u32(tab + Lay::kKi);
     const uint32_t sD = tc::smem_u32(D);
     constexpr uint32_t ID64 = tc::idesc_tf32(128, 64, 0, 0);
@@ -242,80 +255,122 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
         const int n = a.count[g0];
         const bool mine = inrange && n >= G;          // full group: filtered here
         const uint32_t pk = a.pos[g0 * G + j];
+        const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
+        const int b0 = r & ~31;
+        // Region mode (BM3D): every full group of the tile lies in one frame and the bounding box
+        // of its blocks (the same for the three planes) fits a box buffer; the box is then staged
+        // with aligned 16-byte copies and the blocks are cut out of shared memory, and the
+        // aggregation adds into a box before one pass of vector atomics.  Otherwise blocks are
+        // copied and added one by one.
+        int y0 = 0, x0 = 0, rh = 0, rw = 0, frame = 0;
+        bool region = false;
+        if (!a.vbm3d) {
+            const long long f = g0 / a.blocks_per_frame;
+            const int py = unpack_y(pk), px = unpack_x(pk);
+            int ymin = mine ? py : 1 << 30, xmin = mine ? px : 1 << 30;
+            int ymax = mine ? py : -1, xmax = mine ? px : -1;
+            int fmin = mine ? (int)f : 1 << 30, fmax = mine ? (int)f : -1;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
+                xmin = min(xmin, __shfl_xor_sync(0xffffffffu, xmin, o));
+                ymax = max(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
+                xmax = max(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
+                fmin = min(fmin, __shfl_xor_sync(0xffffffffu, fmin, o));
+                fmax = max(fmax, __shfl_xor_sync(0xffffffffu, fmax, o));
+            }
+            if (half == 0 && lane == 0) {
+                int *q = bbx + 8 * (r >> 5);
+                q[0] = ymin; q[1] = xmin; q[2] = ymax; q[3] = xmax; q[4] = fmin; q[5] = fmax;
+            }
+            tc::wg_sync(bar_id, TEAM);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                ymin = min(ymin, bbx[8 * q]); xmin = min(xmin, bbx[8 * q + 1]);
+                ymax = max(ymax, bbx[8 * q + 2]); xmax = max(xmax, bbx[8 * q + 3]);
+                fmin = min(fmin, bbx[8 * q + 4]); fmax = max(fmax, bbx[8 * q + 5]);
+            }
+            if (ymax >= 0 && fmin == fmax) {
+                y0 = ymin;
+                x0 = xmin & ~3;
+                rh = ymax + 8 - ymin;
+                // whole 16-byte chunks, never past the padded row (ld is a multiple of 32)
+                rw = min((xmax + 8 - x0 + 3) & ~3, a.ld - x0);
+                region = rh * rw <= Shp::kRegion;
+                frame = fmin;
+            }
+        }
+        // source and reference boxes of plane pp (three-box form), as asynchronous copies
+        auto load_boxes = [&](int pp) {
+            const long long fo = (long long)frame * a.frame_stride + (long long)y0 * a.ld + x0;
+            const int nv = rh * (rw >> 2);
+            for (int v = t; v < nv; v += TEAM) {
+                const int yy = v / (rw >> 2), c4 = v - yy * (rw >> 2);
+                const long long go = fo + (long long)yy * a.ld + 4 * c4;
+                tc::cp_async16(Bs + yy * rw + 4 * c4, a.src[pp] + go);
+                tc::cp_async16(Br + yy * rw + 4 * c4, a.ref[pp] + go);
+            }
+        };
+        auto next_plane = [&](int pp) {
+            while (pp < 3 && !a.process[pp]) ++pp;
+            return pp;
+        };
+        if constexpr (Shp::kBoxes == 3)
+            if (region && next_plane(0) < 3) load_boxes(next_plane(0));
         for (int p = 0; p < 3 && !failed; ++p) {
             if (!a.process[p]) continue;
             const GroupLoc L = locate(a, p, g0, pk);
-            const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
-            const int b0 = r & ~31;
-            // Region mode (BM3D): every full group of the tile lies in one frame and the bounding
-            // box of its blocks fits the region buffer; the box is then staged once with aligned
-            // 16-byte copies and the blocks are cut out of shared memory, and the aggregation adds
-            // into the same buffer before one pass of vector atomics.  Otherwise blocks are copied
-            // and added one by one.
-            int y0 = 0, x0 = 0, rh = 0, rw = 0, frame = 0;
-            bool region = false;
-            {
-                const long long f = g0 / a.blocks_per_frame;
-                int ymin = mine ? L.y : 1 << 30, xmin = mine ? L.x : 1 << 30;
-                int ymax = mine ? L.y : -1, xmax = mine ? L.x : -1;
-                int fmin = mine ? (int)f : 1 << 30, fmax = mine ? (int)f : -1;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
-                    xmin = min(xmin, __shfl_xor_sync(0xffffffffu, xmin, o));
-                    ymax = max(ymax, __shfl_xor_sync(0xffffffffu, ymax, o));
-                    xmax = max(xmax, __shfl_xor_sync(0xffffffffu, xmax, o));
-                    fmin = min(fmin, __shfl_xor_sync(0xffffffffu, fmin, o));
-                    fmax = max(fmax, __shfl_xor_sync(0xffffffffu, fmax, o));
-                }
-                if (half == 0 && lane == 0) {
-                    int *q = bbx + 8 * (r >> 5);
-                    q[0] = ymin; q[1] = xmin; q[2] = ymax; q[3] = xmax; q[4] = fmin; q[5] = fmax;
-                }
-                tc::wg_sync(bar_id, TEAM);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    ymin = min(ymin, bbx[8 * q]); xmin = min(xmin, bbx[8 * q + 1]);
-                    ymax = max(ymax, bbx[8 * q + 2]); xmax = max(xmax, bbx[8 * q + 3]);
-                    fmin = min(fmin, bbx[8 * q + 4]); fmax = max(fmax, bbx[8 * q + 5]);
-                }
-                if (!a.vbm3d && ymax >= 0 && fmin == fmax) {
-                    y0 = ymin;
-                    x0 = xmin & ~3;
-                    rh = ymax + 8 - ymin;
-                    // whole 16-byte chunks, never past the padded row (ld is a multiple of 32)
-                    rw = min((xmax + 8 - x0 + 3) & ~3, a.ld - x0);
-                    region = rh * rw <= Shp::kRegion;
-                    frame = fmin;
-                }
-            }
             // 1. gather (rows of foreign or partial groups are zero), one block per warp step
             if (region) {
-                const long long fo = (long long)frame * a.frame_stride;
-                const int nv = rh * (rw >> 2);
-                for (int pass = WIENER ? 0 : 1; pass < 2; ++pass) {
-                    // pass 0: reference plane -> R; pass 1: source plane -> X
-                    const float *plane = (pass == 0 ? a.ref[p] : a.src[p]) + fo + (long long)y0 * a.ld + x0;
-                    unsigned char *dst = D + (pass == 0 ? Lay::kXBytes : 0);
-                    for (int v = t; v < nv; v += TEAM) {
-                        const int yy = v / (rw >> 2), c4 = v - yy * (rw >> 2);
-                        tc::cp_async16(Rg + yy * rw + 4 * c4, plane + (long long)yy * a.ld + 4 * c4);
-                    }
+                if constexpr (Shp::kBoxes == 3) {
                     tc::cp_async_wait_all();
                     tc::wg_sync(bar_id, TEAM);
 #pragma unroll 4
                     for (int i = half * NI; i < half * NI + NI; ++i) {
                         const bool mi = __shfl_sync(0xffffffffu, mine, i);
                         const int by = __shfl_sync(0xffffffffu, L.y, i) - y0, bx = __shfl_sync(0xffffffffu, L.x, i) - x0;
-                        float v0 = 0.f, v1 = 0.f;
+                        float v0 = 0.f, v1 = 0.f, u0 = 0.f, u1 = 0.f;
                         if (mi) {
-                            v0 = Rg[(by + ry) * rw + bx + cx];
-                            v1 = Rg[(by + ry + 4) * rw + bx + cx];
+                            v0 = Bs[(by + ry) * rw + bx + cx];
+                            v1 = Bs[(by + ry + 4) * rw + bx + cx];
+                            u0 = Br[(by + ry) * rw + bx + cx];
+                            u1 = Br[(by + ry + 4) * rw + bx + cx];
                         }
-                        *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane, 128)) = v0;
-                        *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
+                        *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128)) = v0;
+                        *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
+                        *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128)) = u0;
+                        *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane + 32, 128)) = u1;
                     }
                     tc::wg_sync(bar_id, TEAM);
+                    // the next plane's boxes load while this plane is filtered
+                    if (next_plane(p + 1) < 3) load_boxes(next_plane(p + 1));
+                } else {
+                    const long long fo = (long long)frame * a.frame_stride;
+                    const int nv = rh * (rw >> 2);
+                    for (int pass = WIENER ? 0 : 1; pass < 2; ++pass) {
+                        // pass 0: reference plane -> R; pass 1: source plane -> X
+                        const float *plane = (pass == 0 ? a.ref[p] : a.src[p]) + fo + (long long)y0 * a.ld + x0;
+                        unsigned char *dst = D + (pass == 0 ? Lay::kXBytes : 0);
+                        for (int v = t; v < nv; v += TEAM) {
+                            const int yy = v / (rw >> 2), c4 = v - yy * (rw >> 2);
+                            tc::cp_async16(Rg + yy * rw + 4 * c4, plane + (long long)yy * a.ld + 4 * c4);
+                        }
+                        tc::cp_async_wait_all();
+                        tc::wg_sync(bar_id, TEAM);
+#pragma unroll 4
+                        for (int i = half * NI; i < half * NI + NI; ++i) {
+                            const bool mi = __shfl_sync(0xffffffffu, mine, i);
+                            const int by = __shfl_sync(0xffffffffu, L.y, i) - y0, bx = __shfl_sync(0xffffffffu, L.x, i) - x0;
+                            float v0 = 0.f, v1 = 0.f;
+                            if (mi) {
+                                v0 = Rg[(by + ry) * rw + bx + cx];
+                                v1 = Rg[(by + ry + 4) * rw + bx + cx];
+                            }
+                            *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane, 128)) = v0;
+                            *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
+                        }
+                        tc::wg_sync(bar_id, TEAM);
+                    }
                 }
             } else {
                 const float *sp = L.src + (long long)L.y * a.ld + L.x;
@@ -450,7 +505,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 for (int o = 16; o > 0; o >>= 1) cmax = fmaxf(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
                 if ((t & 31) == 0) reinterpret_cast<float *>(bbx)[t >> 5] = cmax;
                 int *Ri = reinterpret_cast<int *>(Rg);
-                if (region)
+                if (Shp::kBoxes == 1 && region)           // (the three-box form clears it in the flush)
                     for (int e = t; e < rh * rw; e += TEAM) Ri[e] = 0;
                 tc::wg_sync(bar_id, TEAM);
                 float scale = 1073741824.0f;                 // 2^30
@@ -500,6 +555,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                             const float inv = 1.0f / scale;
                             const float4 q = make_float4((float)qi.x * inv, (float)qi.y * inv, (float)qi.z * inv, (float)qi.w * inv);
                             atomicAdd(reinterpret_cast<float4 *>(nbase + (long long)yy * a.ld + 4 * c4), q);
+                            if constexpr (Shp::kBoxes == 3) *reinterpret_cast<int4 *>(Ri + yy * rw + 4 * c4) = make_int4(0, 0, 0, 0);
                         }
                     }
                 }
@@ -510,6 +566,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             tc::fence_after_sync();
         }
     }
+    tc::cp_async_wait_all();                          // no box copy outlives the kernel
     if (failed && t == 0) atomicExch(status, 1);
     tc::fence_before_sync();
     __syncthreads();

@@ -1058,13 +1058,7 @@ public:
             CU(launch_cf_tc(a, tc_tab.p, tc_status.as<int>(), stream));
             a.skip_full = 1;
         }
-        if (fast) {
-            const int GPW = 32 / para.G;
-            const long long warps_needed = (ngroups + GPW - 1) / GPW;
-            const int warps = 4;
-            const long long grid = std::max<long long>(1, std::min<long long>((warps_needed + warps - 1) / warps, 148LL * 64));
-            CU(launch_cf_fast(a, warps, (int)grid, stream));
-        }
+        if (fast) CU(launch_cf_fast(a, stream));
         if (!fast) {
             // generic path: block sizes other than 8 and group sizes outside {8, 16, 32}; one warp
             // per group with a global scratch slot per resident warp (at most 1 GiB in total)

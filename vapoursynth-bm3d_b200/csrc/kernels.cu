@@ -67,24 +67,39 @@ cudaError_t launch_vbm_predict(const VBMArgs &a, int nframes, size_t smem, cudaS
 int cf_fast_supported(int B, int G) { return B == 8 && (G == 8 || G == 16 || G == 32); }
 
 template <int G, bool W>
-static cudaError_t launch_cf_fast_t(const CFArgs &a, int warps, int grid, cudaStream_t s)
+static cudaError_t launch_cf_fast_t(const CFArgs &a, cudaStream_t s)
 {
-    const size_t smem = (size_t)warps * (W ? 2 : 1) * 32 * 65 * sizeof(float);
     cudaError_t e;
+    if constexpr (W) if (!a.skip_full && !a.vbm3d) {
+        // Final over all groups of BM3D frames: runs of consecutive groups, one per CTA
+        const size_t smem = (size_t)kCfWarps * 2 * 32 * kTP * sizeof(float) + kCfCells * sizeof(unsigned long long) +
+                            kCfWarps * 8 * sizeof(int);
+        const long long runs = (a.ngroups + kCfRunGroups - 1) / kCfRunGroups;
+        const int grid = (int)std::max<long long>(1, std::min<long long>(runs, 1LL << 20));
+        if ((e = allow_smem(cf_run_kernel<G, W>, smem)) != cudaSuccess) return e;
+        COUNT_LAUNCH();
+        cf_run_kernel<G, W><<<grid, 32 * kCfWarps, smem, s>>>(a);
+        return cudaGetLastError();
+    }
+    // per-lane kernel: 4 warps per CTA, grid-stride over the groups
+    const int warps = 4;
+    const long long warps_needed = (a.ngroups + (32 / G) - 1) / (32 / G);
+    const int grid = (int)std::max<long long>(1, std::min<long long>((warps_needed + warps - 1) / warps, 148LL * 64));
+    const size_t smem = (size_t)warps * (W ? 2 : 1) * 32 * kTP * sizeof(float);
     if ((e = allow_smem(cf_fast_kernel<G, W>, smem)) != cudaSuccess) return e;
     COUNT_LAUNCH();
     cf_fast_kernel<G, W><<<grid, 32 * warps, smem, s>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_cf_fast(const CFArgs &a, int warps, int grid, cudaStream_t s)
+cudaError_t launch_cf_fast(const CFArgs &a, cudaStream_t s)
 {
     if (a.B != 8) return cudaErrorInvalidValue;
     const bool w = a.wiener != 0;
     switch (a.G) {
-    case 8: return w ? launch_cf_fast_t<8, true>(a, warps, grid, s) : launch_cf_fast_t<8, false>(a, warps, grid, s);
-    case 16: return w ? launch_cf_fast_t<16, true>(a, warps, grid, s) : launch_cf_fast_t<16, false>(a, warps, grid, s);
-    case 32: return w ? launch_cf_fast_t<32, true>(a, warps, grid, s) : launch_cf_fast_t<32, false>(a, warps, grid, s);
+    case 8: return w ? launch_cf_fast_t<8, true>(a, s) : launch_cf_fast_t<8, false>(a, s);
+    case 16: return w ? launch_cf_fast_t<16, true>(a, s) : launch_cf_fast_t<16, false>(a, s);
+    case 32: return w ? launch_cf_fast_t<32, true>(a, s) : launch_cf_fast_t<32, false>(a, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -143,6 +158,8 @@ template <int G, bool W>
 static cudaError_t launch_cf_tc_t(const CFArgs &a, const void *tables, int *status, cudaStream_t s)
 {
     using Shp = TcShape<G, W>;
+    // 227 KB per CTA, less the kernel's 1 KB of static shared memory (barriers, aligned)
+    static_assert(Shp::kSmem <= 232448 - 1024, "tensor-core filter: shared memory over the per-CTA limit");
     const size_t smem = (size_t)Shp::kSmem;
     cudaError_t e;
     if ((e = allow_smem(cf_tc_kernel<G, W>, smem)) != cudaSuccess) return e;

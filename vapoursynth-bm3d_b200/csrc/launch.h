@@ -13,9 +13,9 @@ cudaError_t upload_odd_tables(const float *host_odd_all);
 
 cudaError_t launch_bm_full(const BMArgs &a, int nframes, size_t smem_bytes, cudaStream_t s);
 cudaError_t launch_vbm_predict(const VBMArgs &a, int nframes, size_t smem_bytes, cudaStream_t s);
-// Fast collaborative filter (B = 8, G in {8, 16, 32}, any group length n <= G); returns
-// cudaErrorInvalidValue for other shapes.
-cudaError_t launch_cf_fast(const CFArgs &a, int warps, int grid, cudaStream_t s);
+// Fast collaborative filter (B = 8, G in {8, 16, 32}, any group length n <= G); sizes its own
+// grid (one CTA per run of consecutive groups); returns cudaErrorInvalidValue for other shapes.
+cudaError_t launch_cf_fast(const CFArgs &a, cudaStream_t s);
 cudaError_t launch_cf_generic(const CFArgs &a, int warps, int grid, cudaStream_t s);
 cudaError_t launch_convert(const ConvProgram &pr, const PlanePtr *in_dev, const PlanePtr *out_dev,
                            int nframes, cudaStream_t s);

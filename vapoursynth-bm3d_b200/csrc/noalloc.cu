@@ -285,9 +285,7 @@ extern "C" BM3D_API int bm3d_basic_noalloc(const float *src, float *dst, int wid
     ca.slots = 1;
     ca.dtab_off = reinterpret_cast<const int *>(base);
     ca.dtab = base + kOffFloats;
-    const long long warps_needed = (nb + (32 / G) - 1) / (32 / G);
-    const long long grid = std::max<long long>(1, std::min<long long>((warps_needed + 3) / 4, 148LL * 64));
-    if ((e = launch_cf_fast(ca, 4, (int)grid, s)) != cudaSuccess) return set_error(BM3D_ERR_CUDA, cuda_text("collaborative filter", e));
+    if ((e = launch_cf_fast(ca, s)) != cudaSuccess) return set_error(BM3D_ERR_CUDA, cuda_text("collaborative filter", e));
 
     // normalisation in place, then the plane out to the caller
     FinalizeArgs fa{};

@@ -187,6 +187,11 @@ BM3D_API int bm3d_debug_reference_fp64(bm3d_filter *filter, int k, double *plane
 BM3D_API int64_t bm3d_debug_launch_count(void);
 /* Number of reference blocks that took the exact tie-resolution path in the last call. */
 BM3D_API int64_t bm3d_debug_slow_blocks(bm3d_filter *filter);
+/* Precision form ("tf32") block matching of the last call: reference blocks whose tensor-core
+ * distance estimates could not settle the list (all distances then computed exactly), and CTAs
+ * whose tensor-core wait timed out (their blocks also computed exactly).  No reference
+ * counterpart.  Returns 0, or -1 for a null filter. */
+BM3D_API int bm3d_debug_bm_tc_counts(bm3d_filter *filter, int64_t *fallbacks, int64_t *timeouts);
 /* In-place 3-D transform of ngroups groups of n blocks of B x B floats in HOST memory (layout
  * [group][z][y][x]) using the device code of the collaborative filter; fast = 1 selects the
  * register path of the 8x8 / n in {8,16,32} kernels.  inverse = 0 forward (REDFT10 definition),

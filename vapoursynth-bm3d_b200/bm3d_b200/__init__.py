@@ -311,6 +311,13 @@ class FilterNode(VideoNode):
     def slow_blocks(self):
         return int(capi.lib().bm3d_debug_slow_blocks(self._h))
 
+    def bm_tc_counts(self):
+        """Precision-form block matching of the last call: (reference blocks that fell back to
+        exact distances for every candidate, CTAs whose tensor-core wait timed out)."""
+        fb, to = C.c_int64(0), C.c_int64(0)
+        capi.lib().bm3d_debug_bm_tc_counts(self._h, C.byref(fb), C.byref(to))
+        return int(fb.value), int(to.value)
+
 
 class _Namespace:
     def __getattr__(self, name):

@@ -14,8 +14,12 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libbm3d_b200.so")
 SOURCES = ["kernels.cu", "host.cpp", "noalloc.cu"]
-DEPS = SOURCES + ["args.h", "bm.cuh", "cf.cuh", "cf_tc.cuh", "tc.cuh", "common.cuh", "convert.cuh", "launch.h", "params.h",
-                  "select.cuh", "vbm.cuh", os.path.join("..", "..", "include", "bm3d_b200.h")]
+
+
+def deps():
+    """Every source and header of csrc/ plus the public header."""
+    names = [n for n in os.listdir(CSRC) if n.endswith((".cu", ".cuh", ".cpp", ".h"))]
+    return [os.path.join(CSRC, n) for n in names] + [os.path.join(os.path.dirname(HERE), "include", "bm3d_b200.h")]
 
 
 def nvcc_path():
@@ -29,7 +33,7 @@ def needs_build():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    return any(os.path.getmtime(os.path.join(CSRC, d)) > t for d in DEPS)
+    return any(os.path.getmtime(d) > t for d in deps())
 
 
 def build(force=False, verbose=False):

@@ -34,6 +34,45 @@ BM3D_HD inline int vbm_warp_floats(int sp_cap, int list_cap, int G, int ps_num, 
     return 3 * sp_cap + 4 * list_cap + 2 * G + ps_num + B * B;
 }
 
+// Precision-form block matching (bm_tc_kernel): at most kBmtRefs reference blocks per CTA and
+// kBmtCols candidate columns (the union of their search windows along the row).
+constexpr int kBmtRefs = 8;
+constexpr int kBmtCols = 64;
+
+// Shared-memory layout of bm_tc_kernel for a search range (candidate step 1), plane height and
+// reference block step.
+struct BmtLayout {
+    int wh;           // window rows (<= 2 range + 8)
+    int wp;           // window pitch in floats (odd)
+    int nr;           // candidate rows (<= 2 range + 1)
+    int cs;           // per-reference distance slots (>= (2 range + 1)^2 + 1, even)
+    int nrc;          // reference blocks per CTA (their windows span <= kBmtCols columns)
+    int offU, offR, offWin, offNb, offSd, offScr, bytes;
+};
+
+// nrc = 0: the range is too wide for the form
+inline BmtLayout bmt_layout(int range, int H, int block_step)
+{
+    BmtLayout L{};
+    const int span = 2 * range + 1;
+    L.nrc = span > kBmtCols ? 0 : (kBmtCols - span) / block_step + 1;
+    if (L.nrc > kBmtRefs) L.nrc = kBmtRefs;
+    L.nr = span < H - 7 ? span : H - 7;
+    L.wh = L.nr + 7;
+    L.wp = (kBmtCols + 7) | 1;
+    L.cs = (span * span + 1 + 1) & ~1;
+    int o = 0;
+    L.offU = o;   o += (L.wh + 1) * kBmtCols * 16;           // fp16 candidate rows (+1 zero row)
+    L.offR = o;   o += 16 * 64 * 2;                          // reference blocks: high terms, low terms
+    L.offWin = o; o += (L.wh * L.wp * 4 + 15) & ~15;         // fp32 window
+    L.offNb = o;  o += L.nr * kBmtCols * 4;                  // candidate block norms
+    const int sd = kBmtRefs * L.cs * 4, rs = L.wh * kBmtCols * 4;
+    L.offSd = o;  o += sd > rs ? sd : rs;                    // distances (first: row sums of squares)
+    L.offScr = o; o += kBmtRefs * 192 * 4;                   // per-warp selection scratch
+    L.bytes = o;
+    return L;
+}
+
 enum SampleKind : int { SK_U8 = 0, SK_U16 = 1, SK_F32 = 2 };
 
 struct BMArgs {

@@ -236,6 +236,90 @@ __device__ __forceinline__ void add_sq2(float (&acc)[4], int p, f32x2 d)
     acc[2 * p + 1] = __fadd_rn(acc[2 * p + 1], hi);
 }
 
+// Exact SSD (the reference's order) of the 8 x 8 reference block at rp (window, pitch wp) against
+// every lattice candidate (rows t + ry s, columns l + c s; window origin wy0, wx0) into
+// sd[ry * ncols + c], and against the trailing (0, 0) candidate of `plane` into sd[nrows * ncols].
+// One warp.
+__device__ __forceinline__ void ssd8_lattice(float *sd, const float *win, int wp, int wy0, int wx0, const float *rp,
+                                             int t, int l, int s, int nrows, int ncols, const float *plane, long long ld)
+{
+    const int lane = (int)lane_id();
+    const int clat = nrows * ncols;
+    // reference block as packed pairs: rbp[y * 4 + m] = (rb[y][2m], rb[y][2m + 1])
+    f32x2 rbp[32];
+#pragma unroll
+    for (int y = 0; y < 8; ++y)
+#pragma unroll
+        for (int m = 0; m < 4; ++m) rbp[y * 4 + m] = pack2(rp[y * wp + 2 * m], rp[y * wp + 2 * m + 1]);
+
+    // item = 4 horizontally adjacent candidates; consecutive lanes take consecutive rows of
+    // the same quad column (with the odd window pitch their loads hit distinct banks)
+    const int nq = (ncols + 3) >> 2;
+    const int items = nrows * nq;
+    for (int it = lane; it < items; it += 32) {
+        const int q = it / nrows;
+        const int ry = it - q * nrows;
+        const int cy = t + ry * s;
+        const int cx0 = l + 4 * q * s;
+        float acc[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[u][k] = 0.0f;
+        const float *wr = win + (cy - wy0) * wp + (cx0 - wx0);
+        if (s == 1) {
+#pragma unroll
+            for (int y = 0; y < 8; ++y) {
+                float w[11];
+#pragma unroll
+                for (int k = 0; k < 11; ++k) w[k] = wr[y * wp + k];
+                // window pairs starting at even (E) and odd (O) columns
+                f32x2 E[5], O[5];
+#pragma unroll
+                for (int m = 0; m < 5; ++m) {
+                    E[m] = pack2(w[2 * m], w[2 * m + 1]);
+                    O[m] = pack2(w[2 * m + 1], w[2 * m + 2]);
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const f32x2 *Wp = (u & 1) ? O : E;
+                    const int m0 = u >> 1;
+                    // columns 0..3 (lane k takes column k), then 4..7 (lane k takes 4 + k)
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) add_sq2(acc[u], h & 1, sub2(rbp[y * 4 + h], Wp[m0 + h]));
+                }
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (4 * q + u >= ncols) break;
+                const float *wu = wr + u * s;
+#pragma unroll
+                for (int y = 0; y < 8; ++y) {
+#pragma unroll
+                    for (int h = 0; h < 4; ++h)
+                        add_sq2(acc[u], h & 1, sub2(rbp[y * 4 + h], pack2(wu[y * wp + 2 * h], wu[y * wp + 2 * h + 1])));
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c = 4 * q + u;
+            if (c < ncols) sd[ry * ncols + c] = lane_combine(acc[u]);
+        }
+    }
+    if (lane == 0) {
+        // the trailing (0, 0) candidate, read from global memory
+        float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        for (int y = 0; y < 8; ++y) {
+            const float *g = plane + (long long)y * ld;
+#pragma unroll
+            for (int h = 0; h < 4; ++h) add_sq2(acc, h & 1, sub2(rbp[y * 4 + h], pack2(__ldg(g + 2 * h), __ldg(g + 2 * h + 1))));
+        }
+        sd[clat] = lane_combine(acc);
+    }
+}
+
 template <int BT>
 __global__ void __launch_bounds__(256) bm_full_kernel(BMArgs a)
 {
@@ -298,80 +382,7 @@ __global__ void __launch_bounds__(256) bm_full_kernel(BMArgs a)
     const int ctot = clat + 1;
 
     if constexpr (BT == 8) {
-        // reference block as packed pairs: rbp[y * 4 + m] = (rb[y][2m], rb[y][2m + 1])
-        f32x2 rbp[32];
-        const float *rp = win + (j - wy0) * wp + (i - wx0);
-#pragma unroll
-        for (int y = 0; y < 8; ++y)
-#pragma unroll
-            for (int m = 0; m < 4; ++m) rbp[y * 4 + m] = pack2(rp[y * wp + 2 * m], rp[y * wp + 2 * m + 1]);
-
-        // item = 4 horizontally adjacent candidates; consecutive lanes take consecutive rows of
-        // the same quad column (with the odd window pitch their loads hit distinct banks)
-        const int nq = (ncols + 3) >> 2;
-        const int items = nrows * nq;
-        for (int it = lane; it < items; it += 32) {
-            const int q = it / nrows;
-            const int ry = it - q * nrows;
-            const int cy = t + ry * s;
-            const int cx0 = l + 4 * q * s;
-            float acc[4][4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-                for (int k = 0; k < 4; ++k) acc[u][k] = 0.0f;
-            const float *wr = win + (cy - wy0) * wp + (cx0 - wx0);
-            if (s == 1) {
-#pragma unroll
-                for (int y = 0; y < 8; ++y) {
-                    float w[11];
-#pragma unroll
-                    for (int k = 0; k < 11; ++k) w[k] = wr[y * wp + k];
-                    // window pairs starting at even (E) and odd (O) columns
-                    f32x2 E[5], O[5];
-#pragma unroll
-                    for (int m = 0; m < 5; ++m) {
-                        E[m] = pack2(w[2 * m], w[2 * m + 1]);
-                        O[m] = pack2(w[2 * m + 1], w[2 * m + 2]);
-                    }
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const f32x2 *Wp = (u & 1) ? O : E;
-                        const int m0 = u >> 1;
-                        // columns 0..3 (lane k takes column k), then 4..7 (lane k takes 4 + k)
-#pragma unroll
-                        for (int h = 0; h < 4; ++h) add_sq2(acc[u], h & 1, sub2(rbp[y * 4 + h], Wp[m0 + h]));
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    if (4 * q + u >= ncols) break;
-                    const float *wu = wr + u * s;
-#pragma unroll
-                    for (int y = 0; y < 8; ++y) {
-#pragma unroll
-                        for (int h = 0; h < 4; ++h)
-                            add_sq2(acc[u], h & 1, sub2(rbp[y * 4 + h], pack2(wu[y * wp + 2 * h], wu[y * wp + 2 * h + 1])));
-                    }
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int c = 4 * q + u;
-                if (c < ncols) sd[ry * ncols + c] = lane_combine(acc[u]);
-            }
-        }
-        if (lane == 0) {
-            // the trailing (0, 0) candidate, read from global memory
-            float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-            for (int y = 0; y < 8; ++y) {
-                const float *g = plane + (long long)y * a.ld;
-#pragma unroll
-                for (int h = 0; h < 4; ++h) add_sq2(acc, h & 1, sub2(rbp[y * 4 + h], pack2(__ldg(g + 2 * h), __ldg(g + 2 * h + 1))));
-            }
-            sd[clat] = lane_combine(acc);
-        }
+        ssd8_lattice(sd, win, wp, wy0, wx0, win + (j - wy0) * wp + (i - wx0), t, l, s, nrows, ncols, plane, a.ld);
     } else {
         // generic block size: reference block staged in this warp's shared slice
         float *rblk = hk + 2 * a.G;

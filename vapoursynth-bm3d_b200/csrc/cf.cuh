@@ -462,7 +462,7 @@ __global__ void __launch_bounds__(kCfWarps * 32, 1) cf_run_kernel(CFArgs a)
 
     for (long long run = blockIdx.x; run * RUN * TPG < a.ngroups; run += gridDim.x) {
         // bounds of the blocks the run adds
-        int y0 = 0, x0 = 0, rh = 0, rw = 0, frame = 0;
+        int y0 = 0, x0 = 0, rh = 0, rw = 0, rp = 0, frame = 0;
         bool region = false;
         if (!a.skip_full && !a.vbm3d) {
             int v[6] = {1 << 30, 1 << 30, -1, -1, 1 << 30, -1};
@@ -499,7 +499,8 @@ __global__ void __launch_bounds__(kCfWarps * 32, 1) cf_run_kernel(CFArgs a)
                 x0 = v[1] & ~3;
                 rh = v[2] + 8 - v[0];
                 rw = min((v[3] + 8 - x0 + 3) & ~3, a.ld - x0);    // whole 16-byte chunks within the row
-                region = rh * rw <= kCfCells;
+                rp = rw + ((24 - (rw & 15)) & 15);    // pitch = 8 mod 16 cells: 2 wavefronts per block step
+                region = rh * rp <= kCfCells;
                 frame = v[4];
             }
         }
@@ -638,7 +639,7 @@ __global__ void __launch_bounds__(kCfWarps * 32, 1) cf_run_kernel(CFArgs a)
                                     const float val = T[i * kTP + 32 * h + lane];
                                     const int yy = by + ry + 4 * h, xx = bx + cx;
                                     if (fabsf(val) < kCfFixMax)
-                                        atomicAdd(Rq + yy * rw + xx, (unsigned long long)__float2ll_rn(val * kCfFix));
+                                        atomicAdd(Rq + yy * rp + xx, (unsigned long long)__float2ll_rn(val * kCfFix));
                                     else
                                         atomicAdd(a.num[p] + (long long)frame * a.frame_stride + (long long)(y0 + yy) * a.ld + x0 + xx, val);
                                 }
@@ -664,16 +665,16 @@ __global__ void __launch_bounds__(kCfWarps * 32, 1) cf_run_kernel(CFArgs a)
                 // the box to the numerator plane, then cleared for the next plane / run
                 __syncthreads();
                 float *nbase = a.num[p] + (long long)frame * a.frame_stride + (long long)y0 * a.ld + x0;
-                const int nv = rh * (rw >> 2);
+                // two cells per thread: one 16-byte shared load per lane, contiguous across the warp
+                const int nv = rh * (rw >> 1);
                 for (int e = threadIdx.x; e < nv; e += blockDim.x) {
-                    const int yy = e / (rw >> 2), c4 = e - yy * (rw >> 2);
-                    unsigned long long *cell = Rq + yy * rw + 4 * c4;
-                    const long long q0 = (long long)cell[0], q1 = (long long)cell[1], q2 = (long long)cell[2], q3 = (long long)cell[3];
-                    if (q0 | q1 | q2 | q3) {
-                        atomicAdd(reinterpret_cast<float4 *>(nbase + (long long)yy * a.ld + 4 * c4),
-                                  make_float4(__ll2float_rn(q0) * kCfUnfix, __ll2float_rn(q1) * kCfUnfix,
-                                              __ll2float_rn(q2) * kCfUnfix, __ll2float_rn(q3) * kCfUnfix));
-                        cell[0] = cell[1] = cell[2] = cell[3] = 0ull;
+                    const int yy = e / (rw >> 1), c2 = e - yy * (rw >> 1);
+                    ulonglong2 *cell = reinterpret_cast<ulonglong2 *>(Rq + yy * rp + 2 * c2);
+                    const ulonglong2 q = *cell;
+                    if (q.x | q.y) {
+                        atomicAdd(reinterpret_cast<float2 *>(nbase + (long long)yy * a.ld + 2 * c2),
+                                  make_float2(__ll2float_rn((long long)q.x) * kCfUnfix, __ll2float_rn((long long)q.y) * kCfUnfix));
+                        *cell = make_ulonglong2(0ull, 0ull);
                     }
                 }
                 __syncthreads();

@@ -84,7 +84,7 @@ struct TcShape {
     // plane is filtered; otherwise one box serves the gathers and the aggregation in turn.
     static constexpr int kBoxes = WIENER && kZInTmem ? 3 : 1;
     static constexpr int kRegion = kBoxes == 3 ? 2688 : 3072;   // floats per box
-    static constexpr int kExtra = kPart + kRegion * 4 * kBoxes + 128;   // + [4 quarters][8] ints of bounds
+    static constexpr int kExtra = kPart + kRegion * 4 * kBoxes + 256;   // + 2 x [4 quarters][8] ints of scratch
     static constexpr int kSmem = (kData + kExtra) * kWG + TcLayout<G>::kTableBytes - kTabOff;
 };
 
@@ -128,7 +128,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     float *Rg = reinterpret_cast<float *>(extra + Shp::kPart);         // aggregation box
     float *Bs = Shp::kBoxes == 3 ? Rg + Shp::kRegion : Rg;              // source box
     float *Br = Shp::kBoxes == 3 ? Rg + 2 * Shp::kRegion : Rg;          // reference box
-    int *bbx = reinterpret_cast<int *>(extra + Shp::kPart + Shp::kRegion * 4 * Shp::kBoxes);   // [4 quarters][8]
+    int *bbx = reinterpret_cast<int *>(extra + Shp::kPart + Shp::kRegion * 4 * Shp::kBoxes);   // [4 quarters][8]: maxima
+    int *bnd = bbx + 32;                                                  // [4 quarters][8]: tile bounds
     // table byte b lives at tab + b (b >= kTabOff)
     unsigned char *tab = tsm + (Shp::kData + Shp::kExtra) * NWG - Shp::kTabOff;
 
@@ -247,29 +248,39 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
         for (int e = 0; e < NC; ++e) *reinterpret_cast<float *>(D + tc::sw128_offset(row0 + cb + e, r, nt)) = v[e];
     };
 
-    bool failed = false;
-    for (long long tile = (long long)blockIdx.x * NWG + wg; tile < ntiles && !failed; tile += (long long)gridDim.x * NWG) {
-        const long long grp = tile * GPT + wsub;
-        const bool inrange = grp < a.ngroups;
-        const long long g0 = inrange ? grp : 0;
-        const int n = a.count[g0];
-        const bool mine = inrange && n >= G;          // full group: filtered here
-        const uint32_t pk = a.pos[g0 * G + j];
-        const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
-        const int b0 = r & ~31;
-        // Region mode (BM3D): every full group of the tile lies in one frame and the bounding box
-        // of its blocks (the same for the three planes) fits a box buffer; the box is then staged
-        // with aligned 16-byte copies and the blocks are cut out of shared memory, and the
-        // aggregation adds into a box before one pass of vector atomics.  Otherwise blocks are
-        // copied and added one by one.
-        int y0 = 0, x0 = 0, rh = 0, rw = 0, frame = 0;
-        bool region = false;
+    // A tile as this thread sees it: its row's group and block, and the team's image box.
+    struct Tile {
+        long long g0;
+        uint32_t pk;
+        bool mine;
+        bool region;
+        int y0, x0, rh, rw, rp, frame;   // box origin, rows, width and shared-memory row pitch
+    };
+    const int lane = r & 31, ry = lane >> 3, cx = lane & 7;
+    const int b0 = r & ~31;
+    // Region mode (BM3D): every full group of the tile lies in one frame and the bounding box of
+    // its blocks (the same for the three planes) fits a box buffer; the box is then staged with
+    // aligned 16-byte copies and the blocks are cut out of shared memory, and the aggregation adds
+    // into a box before one pass of vector atomics.  Otherwise blocks are copied and added one by
+    // one.  Every thread of the team calls bound_tile at the same point (it holds a team barrier).
+    auto fetch_tile = [&](long long tl) {
+        Tile T;
+        const long long grp = tl * GPT + wsub;
+        const bool inrange = tl < ntiles && grp < a.ngroups;
+        T.g0 = inrange ? grp : 0;
+        T.mine = inrange && a.count[T.g0] >= G;       // full group: filtered here
+        T.pk = a.pos[T.g0 * G + j];
+        T.region = false;
+        T.y0 = T.x0 = T.rh = T.rw = T.rp = T.frame = 0;
+        return T;
+    };
+    auto bound_tile = [&](Tile &T) {
         if (!a.vbm3d) {
-            const long long f = g0 / a.blocks_per_frame;
-            const int py = unpack_y(pk), px = unpack_x(pk);
-            int ymin = mine ? py : 1 << 30, xmin = mine ? px : 1 << 30;
-            int ymax = mine ? py : -1, xmax = mine ? px : -1;
-            int fmin = mine ? (int)f : 1 << 30, fmax = mine ? (int)f : -1;
+            const long long f = T.g0 / a.blocks_per_frame;
+            const int py = unpack_y(T.pk), px = unpack_x(T.pk);
+            int ymin = T.mine ? py : 1 << 30, xmin = T.mine ? px : 1 << 30;
+            int ymax = T.mine ? py : -1, xmax = T.mine ? px : -1;
+            int fmin = T.mine ? (int)f : 1 << 30, fmax = T.mine ? (int)f : -1;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
@@ -280,46 +291,66 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 fmax = max(fmax, __shfl_xor_sync(0xffffffffu, fmax, o));
             }
             if (half == 0 && lane == 0) {
-                int *q = bbx + 8 * (r >> 5);
+                int *q = bnd + 8 * (r >> 5);
                 q[0] = ymin; q[1] = xmin; q[2] = ymax; q[3] = xmax; q[4] = fmin; q[5] = fmax;
             }
             tc::wg_sync(bar_id, TEAM);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                ymin = min(ymin, bbx[8 * q]); xmin = min(xmin, bbx[8 * q + 1]);
-                ymax = max(ymax, bbx[8 * q + 2]); xmax = max(xmax, bbx[8 * q + 3]);
-                fmin = min(fmin, bbx[8 * q + 4]); fmax = max(fmax, bbx[8 * q + 5]);
+                ymin = min(ymin, bnd[8 * q]); xmin = min(xmin, bnd[8 * q + 1]);
+                ymax = max(ymax, bnd[8 * q + 2]); xmax = max(xmax, bnd[8 * q + 3]);
+                fmin = min(fmin, bnd[8 * q + 4]); fmax = max(fmax, bnd[8 * q + 5]);
             }
             if (ymax >= 0 && fmin == fmax) {
-                y0 = ymin;
-                x0 = xmin & ~3;
-                rh = ymax + 8 - ymin;
+                T.y0 = ymin;
+                T.x0 = xmin & ~3;
+                T.rh = ymax + 8 - ymin;
                 // whole 16-byte chunks, never past the padded row (ld is a multiple of 32)
-                rw = min((xmax + 8 - x0 + 3) & ~3, a.ld - x0);
-                region = rh * rw <= Shp::kRegion;
-                frame = fmin;
+                T.rw = min((xmax + 8 - T.x0 + 3) & ~3, a.ld - T.x0);
+                // pitch = 8 mod 16 words: the 4 rows x 8 columns a warp touches in a block step
+                // fall in 32 distinct banks
+                T.rp = T.rw + ((24 - (T.rw & 15)) & 15);
+                T.region = T.rh * T.rp <= Shp::kRegion;
+                T.frame = fmin;
             }
         }
-        // source and reference boxes of plane pp (three-box form), as asynchronous copies
-        auto load_boxes = [&](int pp) {
-            const long long fo = (long long)frame * a.frame_stride + (long long)y0 * a.ld + x0;
-            const int nv = rh * (rw >> 2);
-            for (int v = t; v < nv; v += TEAM) {
-                const int yy = v / (rw >> 2), c4 = v - yy * (rw >> 2);
-                const long long go = fo + (long long)yy * a.ld + 4 * c4;
-                tc::cp_async16(Bs + yy * rw + 4 * c4, a.src[pp] + go);
-                tc::cp_async16(Br + yy * rw + 4 * c4, a.ref[pp] + go);
-            }
-        };
-        auto next_plane = [&](int pp) {
-            while (pp < 3 && !a.process[pp]) ++pp;
-            return pp;
-        };
-        if constexpr (Shp::kBoxes == 3)
-            if (region && next_plane(0) < 3) load_boxes(next_plane(0));
+    };
+    // source and reference boxes of plane pp of tile T (three-box form), as asynchronous copies
+    auto load_boxes = [&](const Tile &T, int pp) {
+        const long long fo = (long long)T.frame * a.frame_stride + (long long)T.y0 * a.ld + T.x0;
+        const int nv = T.rh * (T.rw >> 2);
+        for (int v = t; v < nv; v += TEAM) {
+            const int yy = v / (T.rw >> 2), c4 = v - yy * (T.rw >> 2);
+            const long long go = fo + (long long)yy * a.ld + 4 * c4;
+            tc::cp_async16(Bs + yy * T.rp + 4 * c4, a.src[pp] + go);
+            tc::cp_async16(Br + yy * T.rp + 4 * c4, a.ref[pp] + go);
+        }
+    };
+    auto next_plane = [&](int pp) {
+        while (pp < 3 && !a.process[pp]) ++pp;
+        return pp;
+    };
+    const int pfirst = next_plane(0);
+    const long long tstride = (long long)gridDim.x * NWG;
+
+    bool failed = false;
+    Tile cur = fetch_tile((long long)blockIdx.x * NWG + wg);
+    bound_tile(cur);
+    if constexpr (Shp::kBoxes == 3)
+        if (cur.region && pfirst < 3) load_boxes(cur, pfirst);
+    for (long long tile = (long long)blockIdx.x * NWG + wg; tile < ntiles && !failed; tile += tstride) {
+        // the next tile's bounds (and, in the three-box form, its first boxes) are taken during
+        // the gather of this tile's last plane
+        Tile nxt = fetch_tile(tile + tstride);       // loads in flight during this tile
+        const long long g0 = cur.g0;
+        const bool mine = cur.mine;
+        const uint32_t pk = cur.pk;
+        const bool region = cur.region;
+        const int y0 = cur.y0, x0 = cur.x0, rh = cur.rh, rw = cur.rw, rp = cur.rp, frame = cur.frame;
         for (int p = 0; p < 3 && !failed; ++p) {
             if (!a.process[p]) continue;
             const GroupLoc L = locate(a, p, g0, pk);
+            const bool last = next_plane(p + 1) >= 3;
             // 1. gather (rows of foreign or partial groups are zero), one block per warp step
             if (region) {
                 if constexpr (Shp::kBoxes == 3) {
@@ -331,10 +362,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         const int by = __shfl_sync(0xffffffffu, L.y, i) - y0, bx = __shfl_sync(0xffffffffu, L.x, i) - x0;
                         float v0 = 0.f, v1 = 0.f, u0 = 0.f, u1 = 0.f;
                         if (mi) {
-                            v0 = Bs[(by + ry) * rw + bx + cx];
-                            v1 = Bs[(by + ry + 4) * rw + bx + cx];
-                            u0 = Br[(by + ry) * rw + bx + cx];
-                            u1 = Br[(by + ry + 4) * rw + bx + cx];
+                            v0 = Bs[(by + ry) * rp + bx + cx];
+                            v1 = Bs[(by + ry + 4) * rp + bx + cx];
+                            u0 = Br[(by + ry) * rp + bx + cx];
+                            u1 = Br[(by + ry + 4) * rp + bx + cx];
                         }
                         *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128)) = v0;
                         *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
@@ -343,7 +374,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     }
                     tc::wg_sync(bar_id, TEAM);
                     // the next plane's boxes load while this plane is filtered
-                    if (next_plane(p + 1) < 3) load_boxes(next_plane(p + 1));
+                    if (!last) load_boxes(cur, next_plane(p + 1));
                 } else {
                     const long long fo = (long long)frame * a.frame_stride;
                     const int nv = rh * (rw >> 2);
@@ -353,7 +384,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         unsigned char *dst = D + (pass == 0 ? Lay::kXBytes : 0);
                         for (int v = t; v < nv; v += TEAM) {
                             const int yy = v / (rw >> 2), c4 = v - yy * (rw >> 2);
-                            tc::cp_async16(Rg + yy * rw + 4 * c4, plane + (long long)yy * a.ld + 4 * c4);
+                            tc::cp_async16(Rg + yy * rp + 4 * c4, plane + (long long)yy * a.ld + 4 * c4);
                         }
                         tc::cp_async_wait_all();
                         tc::wg_sync(bar_id, TEAM);
@@ -363,8 +394,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                             const int by = __shfl_sync(0xffffffffu, L.y, i) - y0, bx = __shfl_sync(0xffffffffu, L.x, i) - x0;
                             float v0 = 0.f, v1 = 0.f;
                             if (mi) {
-                                v0 = Rg[(by + ry) * rw + bx + cx];
-                                v1 = Rg[(by + ry + 4) * rw + bx + cx];
+                                v0 = Rg[(by + ry) * rp + bx + cx];
+                                v1 = Rg[(by + ry + 4) * rp + bx + cx];
                             }
                             *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane, 128)) = v0;
                             *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
@@ -400,6 +431,11 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     }
                 }
                 tc::cp_async_wait_all();
+            }
+            if (last) {
+                bound_tile(nxt);
+                if constexpr (Shp::kBoxes == 3)
+                    if (nxt.region) load_boxes(nxt, pfirst);
             }
             publish();
             // 2. 2-D DCT
@@ -506,7 +542,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 if ((t & 31) == 0) reinterpret_cast<float *>(bbx)[t >> 5] = cmax;
                 int *Ri = reinterpret_cast<int *>(Rg);
                 if (Shp::kBoxes == 1 && region)           // (the three-box form clears it in the flush)
-                    for (int e = t; e < rh * rw; e += TEAM) Ri[e] = 0;
+                    for (int e = t; e < rh * rp; e += TEAM) Ri[e] = 0;
                 tc::wg_sync(bar_id, TEAM);
                 float scale = 1073741824.0f;                 // 2^30
                 if (region) {
@@ -530,8 +566,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         if (mi) {
                             const float x0v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane, 128));
                             const float x1v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128));
-                            atomicAdd(Ri + (by + ry) * rw + bx + cx, __float2int_rn(x0v * wi * scale));
-                            atomicAdd(Ri + (by + ry + 4) * rw + bx + cx, __float2int_rn(x1v * wi * scale));
+                            atomicAdd(Ri + (by + ry) * rp + bx + cx, __float2int_rn(x0v * wi * scale));
+                            atomicAdd(Ri + (by + ry + 4) * rp + bx + cx, __float2int_rn(x1v * wi * scale));
                         }
                     } else {
                         float *ni = reinterpret_cast<float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(np), i));
@@ -550,12 +586,12 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     const int nv = rh * (rw >> 2);
                     for (int e = t; e < nv; e += TEAM) {
                         const int yy = e / (rw >> 2), c4 = e - yy * (rw >> 2);
-                        const int4 qi = *reinterpret_cast<const int4 *>(Ri + yy * rw + 4 * c4);
+                        const int4 qi = *reinterpret_cast<const int4 *>(Ri + yy * rp + 4 * c4);
                         if (qi.x != 0 || qi.y != 0 || qi.z != 0 || qi.w != 0) {
                             const float inv = 1.0f / scale;
                             const float4 q = make_float4((float)qi.x * inv, (float)qi.y * inv, (float)qi.z * inv, (float)qi.w * inv);
                             atomicAdd(reinterpret_cast<float4 *>(nbase + (long long)yy * a.ld + 4 * c4), q);
-                            if constexpr (Shp::kBoxes == 3) *reinterpret_cast<int4 *>(Ri + yy * rw + 4 * c4) = make_int4(0, 0, 0, 0);
+                            if constexpr (Shp::kBoxes == 3) *reinterpret_cast<int4 *>(Ri + yy * rp + 4 * c4) = make_int4(0, 0, 0, 0);
                         }
                     }
                 }
@@ -565,6 +601,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             tc::wg_sync(bar_id, TEAM);
             tc::fence_after_sync();
         }
+        cur = nxt;
     }
     tc::cp_async_wait_all();                          // no box copy outlives the kernel
     if (failed && t == 0) atomicExch(status, 1);

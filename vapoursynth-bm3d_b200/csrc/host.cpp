@@ -539,8 +539,10 @@ public:
     bool rdef = false;
     cudaStream_t stream = nullptr;
     cudaStream_t own = nullptr;
-    unsigned long long *stats = nullptr;
+    unsigned long long *stats = nullptr;      // [0] exact-heap selections, [1] precision-form matching
+                                              // fallbacks, [2] precision-form tensor-core time-outs
     unsigned long long last_slow = 0;
+    unsigned long long last_stats[3] = {0, 0, 0};
     // stage timing (CUDA events on the filter's stream): 0 ingest, 1 block matching,
     // 2 predictive search, 3 collaborative filter + aggregation, 4 normalise / stack, 5 egress
     static constexpr int kStages = 6;
@@ -581,12 +583,18 @@ public:
     virtual int reference_fp64(int, double *, long long) { return -1; }
     // called after the filter's stream was synchronised (device-side error flags)
     virtual void synced() {}
+    // the stats counters after the stream was synchronised
+    void read_stats()
+    {
+        CU(cudaMemcpy(last_stats, stats, sizeof(last_stats), cudaMemcpyDeviceToHost));
+        last_slow = last_stats[0];
+    }
     int nplanes() const { return vi.color_family == BM3D_GRAY ? 1 : 3; }
     void init_stream()
     {
         CU(cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking));
         stream = own;
-        CU(cudaMalloc(&stats, sizeof(unsigned long long)));
+        CU(cudaMalloc(&stats, 3 * sizeof(unsigned long long)));
     }
 
 protected:
@@ -890,7 +898,7 @@ public:
 
     void synced() override
     {
-        CU(cudaMemcpy(&last_slow, stats, sizeof(last_slow), cudaMemcpyDeviceToHost));
+        read_stats();
         check_tc_status();
     }
 
@@ -999,6 +1007,14 @@ public:
         const int lat = (2 * a.range / a.step + 1);
         a.cand_cap = lat * lat + 1;
         a.win_h = std::min(H, 2 * a.range + a.B);
+        if (tc && para.B == 8 && a.step == 1 && para.G >= 2 && para.G <= 32) {
+            // precision form: distance estimates on the tensor cores, exact lists
+            const BmtLayout L = bmt_layout(a.range, H, para.step);
+            if (L.nrc >= 1 && L.bytes <= 200 * 1024) {
+                CU(launch_bm_tc(a, L, nout, stream));
+                return;
+            }
+        }
         size_t smem = 0;
         int warps = 8;
         for (; warps >= 1; warps /= 2) {
@@ -1198,7 +1214,7 @@ public:
                 acc_num[p].get(sizeof(float) * fs * count);
                 acc_w[p].get(sizeof(float) * fs * count);
             }
-        CU(cudaMemsetAsync(stats, 0, sizeof(unsigned long long), stream));
+        CU(cudaMemsetAsync(stats, 0, 3 * sizeof(unsigned long long), stream));
         mark(0);
         std::vector<bool> full(count);
         for (int k = 0; k < count; ++k) {
@@ -1270,7 +1286,7 @@ public:
         last_count = count;
         if (sync) {
             CU(cudaStreamSynchronize(stream));
-            CU(cudaMemcpy(&last_slow, stats, sizeof(last_slow), cudaMemcpyDeviceToHost));
+            read_stats();
             check_tc_status();
             stager_.release();
         }
@@ -1334,7 +1350,7 @@ public:
                 acc_num[p].get(sizeof(float) * fs * slots * count);
                 acc_w[p].get(sizeof(float) * fs * slots * count);
             }
-        CU(cudaMemsetAsync(stats, 0, sizeof(unsigned long long), stream));
+        CU(cudaMemsetAsync(stats, 0, 3 * sizeof(unsigned long long), stream));
         // window frames into the workspace; properties of each output frame's own source frame
         std::vector<bool> full(nwin);
         for (int i = 0; i < nwin; ++i) full[i] = true;
@@ -1458,7 +1474,7 @@ public:
         last_count = count;
         if (sync) {
             CU(cudaStreamSynchronize(stream));
-            CU(cudaMemcpy(&last_slow, stats, sizeof(last_slow), cudaMemcpyDeviceToHost));
+            read_stats();
             check_tc_status();
             stager_.release();
         }
@@ -1869,6 +1885,14 @@ BM3D_API int64_t bm3d_debug_slow_blocks(bm3d_filter *h)
 {
     if (!h) return -1;
     return (int64_t)h->f->last_slow;
+}
+
+BM3D_API int bm3d_debug_bm_tc_counts(bm3d_filter *h, int64_t *fallbacks, int64_t *timeouts)
+{
+    if (!h) return -1;
+    if (fallbacks) *fallbacks = (int64_t)h->f->last_stats[1];
+    if (timeouts) *timeouts = (int64_t)h->f->last_stats[2];
+    return 0;
 }
 
 BM3D_API int bm3d_debug_dct3d(float *groups, int ngroups, int n, int B, int inverse, int fast)

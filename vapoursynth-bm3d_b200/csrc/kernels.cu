@@ -4,6 +4,7 @@
 #include "common.cuh"
 #include "select.cuh"
 #include "bm.cuh"
+#include "bm_tc.cuh"
 #include "vbm.cuh"
 #include "cf.cuh"
 #include "cf_tc.cuh"
@@ -34,6 +35,18 @@ static cudaError_t allow_smem(K kernel, size_t bytes)
 {
     if (bytes <= 48 * 1024) return cudaSuccess;
     return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+cudaError_t launch_bm_tc(const BMArgs &a, const BmtLayout &L, int nframes, cudaStream_t s)
+{
+    dim3 grid((a.nbx + L.nrc - 1) / L.nrc, a.nby, nframes);
+    // at most two CTAs per SM, so that their 256 tensor-memory columns each are never contended
+    const size_t smem = std::max<size_t>((size_t)L.bytes, 76 * 1024);
+    cudaError_t e;
+    if ((e = allow_smem(bm_tc_kernel, smem)) != cudaSuccess) return e;
+    COUNT_LAUNCH();
+    bm_tc_kernel<<<grid, kBmtThreads, smem, s>>>(a, L);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_bm_full(const BMArgs &a, int nframes, size_t smem, cudaStream_t s)

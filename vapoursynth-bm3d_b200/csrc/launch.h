@@ -12,6 +12,9 @@ namespace bm3d {
 cudaError_t upload_odd_tables(const float *host_odd_all);
 
 cudaError_t launch_bm_full(const BMArgs &a, int nframes, size_t smem_bytes, cudaStream_t s);
+// Precision-form full search (B = 8, candidate step 1, group size <= 32, search windows of
+// L.nrc consecutive reference blocks within 64 candidate columns): same lists as launch_bm_full.
+cudaError_t launch_bm_tc(const BMArgs &a, const BmtLayout &L, int nframes, cudaStream_t s);
 cudaError_t launch_vbm_predict(const VBMArgs &a, int nframes, size_t smem_bytes, cudaStream_t s);
 // Fast collaborative filter (B = 8, G in {8, 16, 32}, any group length n <= G); sizes its own
 // grid (one CTA per run of consecutive groups); returns cudaErrorInvalidValue for other shapes.

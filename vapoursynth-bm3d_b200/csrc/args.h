@@ -47,7 +47,7 @@ struct BmtLayout {
     int nr;           // candidate rows (<= 2 range + 1)
     int cs;           // per-reference distance slots (>= (2 range + 1)^2 + 1, even)
     int nrc;          // reference blocks per CTA (their windows span <= kBmtCols columns)
-    int offU, offR, offWin, offNb, offSd, offScr, bytes;
+    int offU, offR, offWin, offRsq, offSd, offScr, bytes;
 };
 
 // nrc = 0: the range is too wide for the form
@@ -65,9 +65,8 @@ inline BmtLayout bmt_layout(int range, int H, int block_step)
     L.offU = o;   o += (L.wh + 1) * kBmtCols * 16;           // fp16 candidate rows (+1 zero row)
     L.offR = o;   o += 16 * 64 * 2;                          // reference blocks: high terms, low terms
     L.offWin = o; o += (L.wh * L.wp * 4 + 15) & ~15;         // fp32 window
-    L.offNb = o;  o += L.nr * kBmtCols * 4;                  // candidate block norms
-    const int sd = kBmtRefs * L.cs * 4, rs = L.wh * kBmtCols * 4;
-    L.offSd = o;  o += sd > rs ? sd : rs;                    // distances (first: row sums of squares)
+    L.offRsq = o; o += L.wh * kBmtCols * 4;                  // row sums of squares of the candidates
+    L.offSd = o;  o += kBmtRefs * L.cs * 4;                  // distance estimates
     L.offScr = o; o += kBmtRefs * 192 * 4;                   // per-warp selection scratch
     L.bytes = o;
     return L;

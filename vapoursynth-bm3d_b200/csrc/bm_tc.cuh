@@ -115,9 +115,8 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
     unsigned char *U = sm + L.offU;
     unsigned char *Rb = sm + L.offR;
     float *win = reinterpret_cast<float *>(sm + L.offWin);
-    float *nb = reinterpret_cast<float *>(sm + L.offNb);
     float *sdall = reinterpret_cast<float *>(sm + L.offSd);
-    float *rsq = sdall;                                // row sums of squares, before the distances
+    float *rsq = reinterpret_cast<float *>(sm + L.offRsq);   // row sums of squares (centred)
 
     if (warp == 0) tc::tmem_alloc(&tslot, 256);
     if (tid < 2) tc::mbar_init(&mbar[tid], 1);
@@ -225,8 +224,7 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
         for (int o = 16; o > 0; o >>= 1) na_part += __shfl_xor_sync(0xffffffffu, na_part, o);
         if (lane == 0) s_na[n] = na_part;
     }
-    // U and the reference blocks to the tensor cores' view, then the products start while the
-    // block norms are computed
+    // U and the reference blocks to the tensor cores' view
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
@@ -239,38 +237,22 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
     const int nphases = (npairs + kBmtPairsPerPhase - 1) / kBmtPairsPerPhase;
     constexpr uint32_t IDF = idesc_f16(128, 16);
     const uint32_t sU = tc::smem_u32(U), sR = tc::smem_u32(Rb);
+    // descriptors: A = U from image row 2 pp + 2 s4 on (LBO: next image row, SBO: next 8
+    // candidates), B = the reference blocks at K step s4 (LBO: next 8 pixels, SBO: low terms)
+    const uint64_t descA = tc::make_desc(sU, kBmtCols * 16, 128);
+    uint64_t descB[4];
+#pragma unroll
+    for (int s4 = 0; s4 < 4; ++s4) descB[s4] = tc::make_desc(sR + (uint32_t)(s4 * 512), 256, 128);
     auto issue = [&](int ph) {
         for (int pp = ph * kBmtPairsPerPhase; pp < min(npairs, (ph + 1) * kBmtPairsPerPhase); ++pp) {
             const uint32_t d = tm + (uint32_t)((pp % kBmtPairsPerPhase) * 16);
 #pragma unroll
-            for (int s4 = 0; s4 < 4; ++s4) {
-                // image rows 2 pp + 2 s4 and + 1 (lanes 64-127: one row further down)
-                const uint64_t ad = tc::make_desc(sU + (uint32_t)((2 * pp + 2 * s4) * kBmtCols * 16), kBmtCols * 16, 128);
-                const uint64_t bd = tc::make_desc(sR + (uint32_t)(s4 * 512), 256, 128);
-                mma_ss_f16(d, ad, bd, IDF, s4 > 0);
-            }
+            for (int s4 = 0; s4 < 4; ++s4)   // image rows 2 pp + 2 s4 on; start address in 16-byte units
+                mma_ss_f16(d, descA + (uint64_t)((2 * pp + 2 * s4) * kBmtCols), descB[s4], IDF, s4 > 0);
         }
         tc::mma_commit(&mbar[ph & 1]);
     };
     if (tid == 0) issue(0);
-
-    // block norms of the candidates (centred), and their maximum
-    float nbm = 0.0f;
-    for (int e = tid; e < nrows * kBmtCols; e += kBmtThreads) {
-        const int r = e / kBmtCols, m = e - r * kBmtCols;
-        float s = 0.0f;
-#pragma unroll
-        for (int u = 0; u < 8; ++u) s += rsq[(r + u) * kBmtCols + m];
-        nb[r * kBmtCols + m] = s;
-        if (m < ncc) nbm = fmaxf(nbm, s);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) nbm = fmaxf(nbm, __shfl_xor_sync(0xffffffffu, nbm, o));
-    if (lane == 0) red[1][warp] = nbm;
-    __syncthreads();
-    nbm = 0.0f;
-#pragma unroll
-    for (int w = 0; w < kBmtRefs; ++w) nbm = fmaxf(nbm, red[1][w]);
 
     // readout: lane quarter q of the tensor memory; the two warps of a quarter take alternate pairs
     const int q = warp & 3;
@@ -293,9 +275,14 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
         nar[n] = s_na[n];
         selfc[n] = X == s_i[n];
     }
+    float nbm = 0.0f;                                  // largest candidate norm this thread saw
     auto emit = [&](int r, const float (&dv)[16]) {
-        if (r >= nrows) return;
-        const float nbv = nb[r * kBmtCols + m];
+        if (r >= nrows || m >= ncc) return;
+        // centred norm of candidate (r, m): the row sums of squares of its 8 rows
+        float nbv = 0.0f;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) nbv += rsq[(r + u) * kBmtCols + m];
+        nbm = fmaxf(nbm, nbv);
         const bool selfrow = t + r == j;
 #pragma unroll
         for (int n = 0; n < kBmtRefs; ++n) {
@@ -328,8 +315,14 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
     }
     if (warp == 0) tc::tmem_free(tm, 256);              // every load has completed (barrier above)
     if (!ok) atomicExch(&fail_flag, 1);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nbm = fmaxf(nbm, __shfl_xor_sync(0xffffffffu, nbm, o));
+    if (lane == 0) red[1][warp] = nbm;
     __syncthreads();
     const bool tc_failed = fail_flag != 0;
+    nbm = 0.0f;
+#pragma unroll
+    for (int w = 0; w < kBmtRefs; ++w) nbm = fmaxf(nbm, red[1][w]);
 
     // 5. selection, one warp per reference block
     if (warp < nref) {

@@ -389,9 +389,35 @@ def ours_arm(args):
             return float(G), 1.0
         return float(cnt.mean()), float((cnt == G).mean())
 
-    for st in (pipe.basic, pipe.final):
-        L.bm3d_synchronize(st.h)
+    def lists_of(st, G, nb):
+        cnt = np.zeros(nb, np.int32)
+        y = np.zeros(nb * G, np.int32)
+        x = np.zeros(nb * G, np.int32)
+        z = np.zeros(nb * G, np.int32)
+        P = C.POINTER
+        rc = L.bm3d_debug_matches(st.h, 0, cnt.ctypes.data_as(P(C.c_int)), z.ctypes.data_as(P(C.c_int)),
+                                  y.ctypes.data_as(P(C.c_int)), x.ctypes.data_as(P(C.c_int)),
+                                  np.zeros(nb * G, np.float32).ctypes.data_as(P(C.c_float)), nb)
+        return (cnt, y.reshape(nb, G), x.reshape(nb, G)) if rc > 0 else None
+
+    for pp in pipes.values():
+        for st in (pp.basic, pp.final):
+            L.bm3d_synchronize(st.h)
     (nb_mean, nb_full), (nf_mean, nf_full) = mean_n(pipe.basic, 16, nb_b), mean_n(pipe.final, 32, nb_f)
+    # match-list agreement of the two forms' Basic matching on frame 0 (same input plane): the
+    # precision form estimates distances on the tensor cores and re-ranks exactly
+    agree = None
+    la, lb = lists_of(pipes["fp32"].basic, 16, nb_b), lists_of(pipes["tf32"].basic, 16, nb_b)
+    if la is not None and lb is not None:
+        same = (la[0] == lb[0])
+        for k in range(16):
+            same &= ((la[1][:, k] == lb[1][:, k]) & (la[2][:, k] == lb[2][:, k])) | (k >= la[0])
+        agree = float(same.mean())
+    tcfb = {}
+    for name, st in (("basic", pipes["tf32"].basic), ("final", pipes["tf32"].final)):
+        fb, to = C.c_int64(0), C.c_int64(0)
+        L.bm3d_debug_bm_tc_counts(st.h, C.byref(fb), C.byref(to))
+        tcfb[name] = (int(fb.value), int(to.value))
     bm_b, dct_b, _ = algorithmic_work(Wd, Hd, F, 4, 16, nb_mean, False)
     bm_f, dct_f, _ = algorithmic_work(Wd, Hd, F, 3, 32, nf_mean, True)
     stage = R["stage"]
@@ -457,6 +483,9 @@ def ours_arm(args):
                        "final_mean_n": round(nf_mean, 3), "final_full_fraction": round(nf_full, 4),
                        "basic_exact_tie_blocks": int(L.bm3d_debug_slow_blocks(pipe.basic.h)),
                        "final_exact_tie_blocks": int(L.bm3d_debug_slow_blocks(pipe.final.h))},
+            "tc_block_matching": {"basic_list_agreement_vs_fp32": agree,
+                                  "exact_fallback_blocks": {k: v[0] for k, v in tcfb.items()},
+                                  "timeouts": {k: v[1] for k, v in tcfb.items()}},
             "gpu_launches": int(R["launches"]),
             "clocks": clk,
             "quality": {"psnr_in_db": round(psnr_in, 3), "psnr_out_db": round(R["psnr"], 3)},

@@ -198,6 +198,30 @@ BM3D_API int bm3d_debug_bm_tc_counts(bm3d_filter *filter, int64_t *fallbacks, in
  * 1 inverse (REDFT01). */
 BM3D_API int bm3d_debug_dct3d(float *groups, int ngroups, int n, int block_size, int inverse, int fast);
 
+/* ---- Learned block-matching proposal (precision = "learned"); no reference counterpart --------
+ * Network: 3x3 conv 1 -> 16 channels, ReLU, 3x3 conv 16 -> 16, bf16 activations; descriptor of
+ * a block position = the 16 features averaged over its 8x8 block.  Weight vector (2480 floats):
+ * w1[16][9], b1[16], w2[16][16][9], b2[16].  Planes are float GRAY, pitch = width.  All return 0
+ * on success (match: the number of reference blocks) or an error code (bm3d_get_error). */
+/* Copies the built-in (trained) weights; returns their count. */
+BM3D_API int bm3d_proposal_default_weights(float *out, int capacity);
+/* Descriptors [height - 7][width - 7][16] (bf16 values as float) of one plane. */
+BM3D_API int bm3d_proposal_descriptors(const float *frame, int width, int height, const float *weights, float *desc_out);
+/* Mean logistic ranking loss softplus(s_ap - s_an) over triplets (ay, ax, py, px, ny, nx) of block
+ * positions, s = squared descriptor distance, and its gradient with respect to the weights. */
+BM3D_API int bm3d_proposal_gradients(const float *frame, int width, int height, const float *weights, const int *triplets,
+                                     int ntriplets, float *loss, float *grad);
+/* Trains on nframes planes [n][height][width] for iters Adam steps of batch triplets; weights in
+ * (initial) and out (trained); losses[iters] receives the mean loss of every step. */
+BM3D_API int bm3d_proposal_train(const float *frames, int nframes, int width, int height, int iters, int batch, float lr,
+                                 uint64_t seed, float *weights, float *losses);
+/* Match lists of one plane (block step, group size <= 32, range, candidate step 1, SSD threshold):
+ * exhaustive when weights is NULL, else the nprop (<= 64) best candidates by descriptor distance
+ * re-ranked with the exact SSD.  counts[n], ys / xs [n][group_size]; capacity = room for n. */
+BM3D_API int bm3d_proposal_match(const float *frame, int width, int height, const float *weights, int block_step,
+                                 int group_size, int bm_range, float th_sse, int nprop, int *counts, int *ys, int *xs,
+                                 int capacity);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,135 @@
+"""Learned block-matching proposal (precision="learned"): the network's GPU forward and backward
+against the NumPy restatement (oracle/proposal_ref.py), training, group recall of the proposals
+against the exhaustive search, the ablation with untrained weights, and the filter's PSNR.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import proposal_ref as pr
+from bm3d_b200 import _capi as capi
+from bm3d_b200 import core, source, synth
+
+pytestmark = pytest.mark.gpu
+P = C.POINTER
+
+
+def fptr(a):
+    return a.ctypes.data_as(P(C.c_float))
+
+
+def iptr(a):
+    return a.ctypes.data_as(P(C.c_int))
+
+
+def default_weights():
+    w = np.zeros(pr.NW, np.float32)
+    assert capi.lib().bm3d_proposal_default_weights(fptr(w), pr.NW) == pr.NW
+    return w
+
+
+def descriptors(x, w):
+    H, W = x.shape
+    out = np.zeros((H - 7, W - 7, 16), np.float32)
+    assert capi.lib().bm3d_proposal_descriptors(fptr(x), W, H, fptr(w), fptr(out)) == 0
+    return out
+
+
+def gpu_grad(x, w, trip):
+    H, W = x.shape
+    t = np.ascontiguousarray(np.asarray(trip, np.int32).ravel())
+    loss = np.zeros(1, np.float32)
+    g = np.zeros(pr.NW, np.float32)
+    assert capi.lib().bm3d_proposal_gradients(fptr(x), W, H, fptr(w), iptr(t), len(trip), fptr(loss), fptr(g)) == 0
+    return float(loss[0]), g
+
+
+def match(x, w, step, G, R, th, nprop):
+    H, W = x.shape
+    cap = 1 << 16
+    cnt = np.zeros(cap, np.int32)
+    ys = np.zeros(cap * G, np.int32)
+    xs = np.zeros(cap * G, np.int32)
+    n = capi.lib().bm3d_proposal_match(fptr(x), W, H, fptr(w) if w is not None else None, step, G, R, C.c_float(th),
+                                        nprop, iptr(cnt), iptr(ys), iptr(xs), cap)
+    assert n > 0
+    return cnt[:n], ys[:n * G].reshape(n, G), xs[:n * G].reshape(n, G)
+
+
+def recall(got, ref):
+    """Mean over reference blocks of |proposal list ∩ exhaustive list| / |exhaustive list|."""
+    (cg, yg, xg), (cr, yr, xr) = got, ref
+    r = []
+    for b in range(len(cr)):
+        a = set(zip(yr[b, :cr[b]].tolist(), xr[b, :cr[b]].tolist()))
+        s = set(zip(yg[b, :cg[b]].tolist(), xg[b, :cg[b]].tolist()))
+        r.append(len(a & s) / len(a))
+    return float(np.mean(r))
+
+
+def test_descriptors_match_restatement():
+    x = synth.gray_frames(70, 1, 40, 52, 10.0)[0][0, 0].astype(np.float32)
+    w = default_weights()
+    got = descriptors(x, w)
+    _, _, ref = pr.forward(x, w, bf=True)
+    tol = 2.0 ** -7 * np.abs(ref) + 1e-3 * np.abs(ref).max()        # one bf16 step, plus summation order
+    assert np.all(np.abs(got - ref) <= tol)
+
+
+def test_gradients_match_restatement():
+    rng = np.random.default_rng(71)
+    x = synth.gray_frames(71, 1, 36, 44, 10.0)[0][0, 0].astype(np.float32)
+    w = default_weights()
+    trip = [tuple(int(v) for v in (rng.integers(0, 29), rng.integers(0, 37), rng.integers(0, 29), rng.integers(0, 37),
+                                   rng.integers(0, 29), rng.integers(0, 37))) for _ in range(64)]
+    Lg, gg = gpu_grad(x, w, trip)
+    Lr, gr = pr.loss_and_grad(x, w, trip, bf=True)
+    print(f"loss gpu {Lg:.6f} restatement {Lr:.6f}; gradient norm {np.linalg.norm(gr):.4g}, "
+          f"max abs diff {np.abs(gg - gr).max():.3g}")
+    assert abs(Lg - Lr) <= 1e-3 * max(1.0, abs(Lr))
+    assert np.linalg.norm(gg - gr) <= 2e-2 * np.linalg.norm(gr)
+    cos = float(np.dot(gg, gr) / (np.linalg.norm(gg) * np.linalg.norm(gr)))
+    assert cos > 0.999
+
+
+def test_training_lowers_the_loss():
+    frames = np.ascontiguousarray(np.stack([synth.gray_frames(72 + k, 1, 96, 96, 10.0)[0][0, 0] for k in range(2)]),
+                                  np.float32)
+    import train_proposal
+    w0 = train_proposal.init_weights(3)
+    w, losses = train_proposal.train(frames, 60, 512, 3e-3, 3, w0)
+    print(f"loss first 10 {losses[:10].mean():.4f}, last 10 {losses[-10:].mean():.4f}")
+    assert np.isfinite(losses).all()
+    assert losses[-10:].mean() < 0.9 * losses[:10].mean()
+
+
+def test_recall_and_ablation():
+    """Group recall of the learned proposals (2 G candidates) against the exhaustive search; the
+    untrained network (He initialisation) must do worse, a random choice much worse."""
+    import train_proposal
+    x = synth.gray_frames(73, 1, 160, 224, 10.0)[0][0, 0].astype(np.float32)
+    ref = match(x, None, 4, 16, 16, 3.0e38, 32)
+    r_trained = recall(match(x, default_weights(), 4, 16, 16, 3.0e38, 32), ref)
+    r_untrained = recall(match(x, train_proposal.init_weights(1), 4, 16, 16, 3.0e38, 32), ref)
+    print(f"recall (16-lists, 32 proposals of 1089): trained {r_trained:.4f}, untrained {r_untrained:.4f}, "
+          f"random {32 / 1089:.4f}")
+    assert r_trained >= 0.85
+    assert r_trained > r_untrained
+
+
+def test_learned_filter_psnr():
+    nz, clean = synth.gray_frames(74, 2, 160, 224, 10.0)
+
+    def run(prec):
+        clip = source(nz, "GRAY")
+        b = core.bm3d.Basic(clip, profile="np", sigma=10.0, precision=prec)
+        f = core.bm3d.Final(clip, b, profile="np", sigma=10.0, precision=prec)
+        return f.numpy()
+
+    def psnr(o):
+        return 10 * np.log10(1.0 / np.mean((o.astype(np.float64) - clean) ** 2))
+
+    p_exh, p_learn = psnr(run("tf32")), psnr(run("learned"))
+    print(f"PSNR exhaustive (tf32) {p_exh:.4f} dB, learned proposals {p_learn:.4f} dB")
+    assert p_learn >= p_exh - 0.05

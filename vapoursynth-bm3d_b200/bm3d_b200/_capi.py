@@ -17,7 +17,8 @@ EXPORTS = [
     "bm3d_get_frames_async", "bm3d_set_stream", "bm3d_synchronize", "bm3d_free", "bm3d_get_error",
     "bm3d_set_log_callback", "bm3d_debug_matches", "bm3d_debug_slow_blocks", "bm3d_debug_dct3d",
     "bm3d_set_profiling", "bm3d_debug_stage_times", "bm3d_debug_launch_count", "bm3d_basic_noalloc",
-    "bm3d_debug_reference_fp64", "bm3d_debug_bm_tc_counts",
+    "bm3d_debug_reference_fp64", "bm3d_debug_bm_tc_counts", "bm3d_proposal_default_weights",
+    "bm3d_proposal_descriptors", "bm3d_proposal_gradients", "bm3d_proposal_train", "bm3d_proposal_match",
 ]
 
 
@@ -69,6 +70,14 @@ def lib():
     L.bm3d_debug_slow_blocks.argtypes = [C.c_void_p]
     L.bm3d_debug_slow_blocks.restype = C.c_int64
     L.bm3d_debug_bm_tc_counts.argtypes = [C.c_void_p, P(C.c_int64), P(C.c_int64)]
+    L.bm3d_proposal_default_weights.argtypes = [P(C.c_float), C.c_int]
+    L.bm3d_proposal_descriptors.argtypes = [P(C.c_float), C.c_int, C.c_int, P(C.c_float), P(C.c_float)]
+    L.bm3d_proposal_gradients.argtypes = [P(C.c_float), C.c_int, C.c_int, P(C.c_float), P(C.c_int), C.c_int,
+                                          P(C.c_float), P(C.c_float)]
+    L.bm3d_proposal_train.argtypes = [P(C.c_float), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_uint64,
+                                      P(C.c_float), P(C.c_float)]
+    L.bm3d_proposal_match.argtypes = [P(C.c_float), C.c_int, C.c_int, P(C.c_float), C.c_int, C.c_int, C.c_int,
+                                      C.c_float, C.c_int, P(C.c_int), P(C.c_int), P(C.c_int), C.c_int]
     L.bm3d_set_profiling.argtypes = [C.c_void_p, C.c_int]
     L.bm3d_debug_stage_times.argtypes = [C.c_void_p, P(C.c_double), C.c_int]
     L.bm3d_debug_launch_count.restype = C.c_int64

@@ -236,6 +236,28 @@ __device__ __forceinline__ void add_sq2(float (&acc)[4], int p, f32x2 d)
     acc[2 * p + 1] = __fadd_rn(acc[2 * p + 1], hi);
 }
 
+// Exact SSD of the 8 x 8 blocks at r (pitch rs) and w (pitch ws) in the reference's SSE2 order:
+// four lane sums, lane k taking column k and then column 4 + k of every row, combined
+// ((s0 + s1) + s2) + s3; every square and sum separately rounded (the packed kernel's arithmetic).
+__device__ __forceinline__ float exact_ssd8(const float *r, int rs, const float *w, long long ws)
+{
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int y = 0; y < 8; ++y) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float d = __fsub_rn(r[y * rs + k], w[y * ws + k]);
+            acc[k] = __fadd_rn(acc[k], __fmul_rn(d, d));
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float d = __fsub_rn(r[y * rs + 4 + k], w[y * ws + 4 + k]);
+            acc[k] = __fadd_rn(acc[k], __fmul_rn(d, d));
+        }
+    }
+    return lane_combine(acc);
+}
+
 // Exact SSD (the reference's order) of the 8 x 8 reference block at rp (window, pitch wp) against
 // every lattice candidate (rows t + ry s, columns l + c s; window origin wy0, wx0) into
 // sd[ry * ncols + c], and against the trailing (0, 0) candidate of `plane` into sd[nrows * ncols].

@@ -58,28 +58,6 @@ __device__ __forceinline__ void mma_ss_f16(uint32_t d_tmem, uint64_t a_desc, uin
                  ::"r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"((uint32_t)accumulate));
 }
 
-// Exact SSD of the 8 x 8 blocks at r (pitch rs) and w (pitch ws) in the reference's SSE2 order:
-// four lane sums, lane k taking column k and then column 4 + k of every row, combined
-// ((s0 + s1) + s2) + s3; every square and sum separately rounded (the packed kernel's arithmetic).
-__device__ __forceinline__ float exact_ssd8(const float *r, int rs, const float *w, long long ws)
-{
-    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-    for (int y = 0; y < 8; ++y) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const float d = __fsub_rn(r[y * rs + k], w[y * ws + k]);
-            acc[k] = __fadd_rn(acc[k], __fmul_rn(d, d));
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const float d = __fsub_rn(r[y * rs + 4 + k], w[y * ws + 4 + k]);
-            acc[k] = __fadd_rn(acc[k], __fmul_rn(d, d));
-        }
-    }
-    return lane_combine(acc);
-}
-
 __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout L)
 {
     extern __shared__ __align__(1024) unsigned char sm[];

@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "launch.h"
+#include "proposal_weights.h"
 #include "params.h"
 
 namespace bm3d {
@@ -697,6 +698,26 @@ public:
 };
 
 // ---------------------------------------------------------------------------------------------
+// Learned block-matching proposal: device buffers and the descriptor pass
+
+struct PropBuffers {
+    DevBuf hid, feat, rs, desc, grad_d, dF, dH;
+};
+
+// bf16 descriptors [frame][H - 7][W - 7][16] of nframes planes (frame stride fs, pitch ld)
+static void prop_descriptors(const float *planes, long long fs, int ld, int W, int H, int nframes, const float *wt,
+                             PropBuffers &pb, cudaStream_t stream)
+{
+    const size_t px = (size_t)W * H, npos = (size_t)(W - 7) * (H - 7);
+    void *hid = pb.hid.get(2 * 16 * px);
+    void *feat = pb.feat.get(2 * 16 * px);
+    float *rs = static_cast<float *>(pb.rs.get(4 * 16 * (size_t)H * (W - 3)));
+    unsigned char *desc = static_cast<unsigned char *>(pb.desc.get(2 * 16 * npos * nframes));
+    for (int k = 0; k < nframes; ++k)
+        CU(launch_prop_features(planes + (long long)k * fs, ld, W, H, wt, hid, feat, rs, desc + 2 * 16 * npos * k, stream));
+}
+
+// ---------------------------------------------------------------------------------------------
 // Shared state of Basic / Final / VBasic / VFinal
 
 class BM3DBase : public Filter {
@@ -704,6 +725,9 @@ public:
     bool wiener = false;
     bool vbm3d = false;
     bool tc = false;            // precision form: tensor-core transforms (argument "precision")
+    bool learned = false;       // precision "learned": block matching by learned proposals
+    DevBuf prop_wt;             // proposal network weights (device)
+    PropBuffers prop_bufs;
     double plane_sigma[3] = {0, 0, 0};
     Params para, para_default;
     int matrix = MAT_UNSPEC;
@@ -836,7 +860,8 @@ public:
         if (!error) {
             const std::string pr(prec);
             if (pr == "tf32") tc = true;
-            else if (pr != "fp32") return fail(BM3D_ERR_ARG, err("Invalid \"precision\" assigned, must be \"fp32\" or \"tf32\""));
+            else if (pr == "learned") tc = learned = true;
+            else if (pr != "fp32") return fail(BM3D_ERR_ARG, err("Invalid \"precision\" assigned, must be \"fp32\", \"tf32\" or \"learned\""));
         }
         return BM3D_OK;
     }
@@ -1007,7 +1032,8 @@ public:
         const int lat = (2 * a.range / a.step + 1);
         a.cand_cap = lat * lat + 1;
         a.win_h = std::min(H, 2 * a.range + a.B);
-        if (tc && para.B == 8 && a.step == 1 && para.G >= 2 && para.G <= 32) {
+        const bool use_learned = learned && para.B == 8 && para.G >= 2 && para.G <= 32;
+        if (tc && !use_learned && para.B == 8 && a.step == 1 && para.G >= 2 && para.G <= 32) {
             // precision form: distance estimates on the tensor cores, exact lists
             const BmtLayout L = bmt_layout(a.range, H, para.step);
             if (L.nrc >= 1 && L.bytes <= 200 * 1024) {
@@ -1026,6 +1052,17 @@ public:
             if (smem <= 200 * 1024) break;
         }
         if (warps < 1) throw std::runtime_error(err("bm_range / block_size too large for the shared-memory search window"));
+        if (use_learned) {
+            // learned proposals: descriptors of every block position, then the best 2 G (at most
+            // 64) candidates by descriptor distance re-ranked with the exact SSD
+            if (!prop_wt.p) {
+                CU(cudaMemcpy(prop_wt.get(sizeof(float) * kProposalWeightCount), kProposalWeights,
+                              sizeof(float) * kProposalWeightCount, cudaMemcpyHostToDevice));
+            }
+            prop_descriptors(a.ref, fs, ld, W, H, nout, prop_wt.as<float>(), prop_bufs, stream);
+            CU(launch_bm_learned(a, prop_bufs.desc.p, std::min(64, 2 * para.G), nout, smem, stream));
+            return;
+        }
         CU(launch_bm_full(a, nout, smem, stream));
     }
 
@@ -1893,6 +1930,216 @@ BM3D_API int bm3d_debug_bm_tc_counts(bm3d_filter *h, int64_t *fallbacks, int64_t
     if (fallbacks) *fallbacks = (int64_t)h->f->last_stats[1];
     if (timeouts) *timeouts = (int64_t)h->f->last_stats[2];
     return 0;
+}
+
+// ---- learned proposal: training and inspection -------------------------------------------------
+
+// Exhaustive lists (exact SSD, no threshold) of nframes planes for block step `step`, group G,
+// range R, candidate step 1: the training targets and the recall reference.
+static void exhaustive_lists(const float *planes, long long fs, int ld, int W, int H, int nframes, int step, int G, int R,
+                             float thsse, const int *dsy, const int *dsx, int nby, int nbx, uint32_t *pos, int *cnt,
+                             const void *desc, int nprop, cudaStream_t stream)
+{
+    BMArgs a{};
+    a.ref = planes;
+    a.frame_stride = fs;
+    a.ld = ld;
+    a.H = H;
+    a.W = W;
+    a.B = 8;
+    a.range = R;
+    a.step = 1;
+    a.G = G;
+    a.thSSE = thsse;
+    a.distMul = 1.0;
+    a.scan_y = dsy;
+    a.scan_x = dsx;
+    a.nby = nby;
+    a.nbx = nbx;
+    a.out_pos = pos;
+    a.out_n = cnt;
+    a.out_key = nullptr;
+    a.stats = nullptr;
+    a.cand_cap = (2 * R + 1) * (2 * R + 1) + 1;
+    a.win_h = std::min(H, 2 * R + 8);
+    size_t smem = 0;
+    int warps = 8;
+    for (; warps >= 1; warps /= 2) {
+        a.warps = warps;
+        a.win_pitch = (std::min(W, (warps - 1) * step + 2 * R + 8) + 4) | 1;
+        smem = sizeof(float) * ((size_t)a.win_h * a.win_pitch + (size_t)warps * bm_warp_floats(a.cand_cap, G, 8, false));
+        if (smem <= 200 * 1024) break;
+    }
+    if (warps < 1) throw std::runtime_error("bm_range too large");
+    if (desc) CU(launch_bm_learned(a, desc, nprop, nframes, smem, stream));
+    else CU(launch_bm_full(a, nframes, smem, stream));
+}
+
+BM3D_API int bm3d_proposal_default_weights(float *out, int capacity)
+{
+    if (!out || capacity < kProposalWeightCount) return fail(BM3D_ERR_STATE, "bm3d_proposal_default_weights: buffer too small");
+    std::memcpy(out, kProposalWeights, sizeof(float) * kProposalWeightCount);
+    return kProposalWeightCount;
+}
+
+BM3D_API int bm3d_proposal_descriptors(const float *frame, int width, int height, const float *weights, float *desc_out)
+{
+    g_error.clear();
+    if (!frame || !weights || !desc_out || width < 8 || height < 8) return fail(BM3D_ERR_STATE, "bad arguments");
+    return guarded([&]() -> int {
+        DevBuf x, wt;
+        PropBuffers pb;
+        CU(cudaMemcpy(x.get(sizeof(float) * width * height), frame, sizeof(float) * width * height, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(wt.get(sizeof(float) * kProposalWeightCount), weights, sizeof(float) * kProposalWeightCount, cudaMemcpyHostToDevice));
+        prop_descriptors(x.as<float>(), 0, width, width, height, 1, wt.as<float>(), pb, 0);
+        const size_t n = (size_t)16 * (width - 7) * (height - 7);
+        std::vector<uint16_t> h(n);
+        CU(cudaMemcpy(h.data(), pb.desc.p, 2 * n, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < n; ++i) {
+            const uint32_t u = (uint32_t)h[i] << 16;
+            std::memcpy(desc_out + i, &u, 4);
+        }
+        return (int)BM3D_OK;
+    });
+}
+
+// Loss and weight gradients for given triplets (ay, ax, py, px, ny, nx: block positions of one
+// plane, p the candidate that should rank closer): L = mean softplus(s_ap - s_an).
+BM3D_API int bm3d_proposal_gradients(const float *frame, int width, int height, const float *weights, const int *triplets,
+                                     int ntriplets, float *loss, float *grad)
+{
+    g_error.clear();
+    if (!frame || !weights || !triplets || ntriplets < 1 || !loss || !grad || width < 8 || height < 8)
+        return fail(BM3D_ERR_STATE, "bad arguments");
+    return guarded([&]() -> int {
+        const int Wd = width - 7, Hd = height - 7;
+        for (int t = 0; t < 6 * ntriplets; ++t)
+            if (triplets[t] < 0 || triplets[t] >= ((t % 2) ? Wd : Hd)) throw std::runtime_error("triplet position outside the plane");
+        DevBuf x, wt, tr, gD, dF, dH, gw, dl;
+        PropBuffers pb;
+        CU(cudaMemcpy(x.get(sizeof(float) * width * height), frame, sizeof(float) * width * height, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(wt.get(sizeof(float) * kProposalWeightCount), weights, sizeof(float) * kProposalWeightCount, cudaMemcpyHostToDevice));
+        std::vector<int> trh(7 * (size_t)ntriplets);
+        for (int t = 0; t < ntriplets; ++t) {
+            trh[7 * t] = 0;
+            for (int k = 0; k < 6; ++k) trh[7 * t + 1 + k] = triplets[6 * t + k];
+        }
+        if (prop_triplet_bytes() != 7 * (int)sizeof(int)) throw std::runtime_error("triplet layout");
+        CU(cudaMemcpy(tr.get(trh.size() * sizeof(int)), trh.data(), trh.size() * sizeof(int), cudaMemcpyHostToDevice));
+        prop_descriptors(x.as<float>(), 0, width, width, height, 1, wt.as<float>(), pb, 0);
+        const size_t npos = (size_t)Wd * Hd, px = (size_t)width * height;
+        CU(cudaMemset(gD.get(sizeof(float) * 16 * npos), 0, sizeof(float) * 16 * npos));
+        CU(cudaMemset(gw.get(sizeof(float) * kProposalWeightCount), 0, sizeof(float) * kProposalWeightCount));
+        CU(cudaMemset(dl.get(sizeof(float)), 0, sizeof(float)));
+        CU(launch_prop_loss(tr.p, ntriplets, pb.desc.p, (long long)npos, Wd, gD.as<float>(), 1.0f / ntriplets, dl.as<float>(), 0));
+        CU(launch_prop_backward(x.as<float>(), width, width, height, wt.as<float>(), pb.hid.p, gD.as<float>(),
+                                static_cast<float *>(dF.get(sizeof(float) * 16 * px)), static_cast<float *>(dH.get(sizeof(float) * 16 * px)),
+                                gw.as<float>(), 0));
+        CU(cudaDeviceSynchronize());
+        CU(cudaMemcpy(loss, dl.p, sizeof(float), cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(grad, gw.p, sizeof(float) * kProposalWeightCount, cudaMemcpyDeviceToHost));
+        return (int)BM3D_OK;
+    });
+}
+
+// Trains the proposal network on nframes GRAY planes [n][height][width] (host, float): per
+// iteration `batch` triplets (reference block on the block-step-4 lattice, one of the first 16
+// entries of its exhaustive 32-list, and either a later entry or a uniform candidate of its +-16
+// window), logistic ranking loss, Adam.
+// weights: initial values in, trained values out; losses[iters]: the mean loss per iteration.
+BM3D_API int bm3d_proposal_train(const float *frames, int nframes, int width, int height, int iters, int batch, float lr,
+                                 uint64_t seed, float *weights, float *losses)
+{
+    g_error.clear();
+    if (!frames || nframes < 1 || width < 48 || height < 48 || iters < 1 || batch < 1 || !weights || !losses)
+        return fail(BM3D_ERR_STATE, "bad arguments");
+    return guarded([&]() -> int {
+        const int W = width, H = height, Wd = W - 7, Hd = H - 7, G = 32, R = 16, step = 4;
+        const size_t px = (size_t)W * H, npos = (size_t)Wd * Hd;
+        const long long fs = (long long)px;
+        DevBuf x, wt, mo, vo, gw, tr, gD, dF, dH, dl, hidall, feat, rs, desc, lp, ln, dsy, dsx;
+        CU(cudaMemcpy(x.get(sizeof(float) * px * nframes), frames, sizeof(float) * px * nframes, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(wt.get(sizeof(float) * kProposalWeightCount), weights, sizeof(float) * kProposalWeightCount, cudaMemcpyHostToDevice));
+        CU(cudaMemset(mo.get(sizeof(float) * kProposalWeightCount), 0, sizeof(float) * kProposalWeightCount));
+        CU(cudaMemset(vo.get(sizeof(float) * kProposalWeightCount), 0, sizeof(float) * kProposalWeightCount));
+        CU(cudaMemset(dl.get(sizeof(float) * iters), 0, sizeof(float) * iters));
+        const std::vector<int> syh = scan_positions(H, 8, step), sxh = scan_positions(W, 8, step);
+        CU(cudaMemcpy(dsy.get(sizeof(int) * syh.size()), syh.data(), sizeof(int) * syh.size(), cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(dsx.get(sizeof(int) * sxh.size()), sxh.data(), sizeof(int) * sxh.size(), cudaMemcpyHostToDevice));
+        const int nby = (int)syh.size(), nbx = (int)sxh.size();
+        const size_t nb = (size_t)nby * nbx * nframes;
+        exhaustive_lists(x.as<float>(), fs, W, W, H, nframes, step, G, R, 3.0e38f, dsy.as<int>(), dsx.as<int>(), nby, nbx,
+                         static_cast<uint32_t *>(lp.get(sizeof(uint32_t) * nb * G)), static_cast<int *>(ln.get(sizeof(int) * nb)),
+                         nullptr, 0, 0);
+        unsigned char *hid = static_cast<unsigned char *>(hidall.get(2 * 16 * px * nframes));
+        unsigned char *dsc = static_cast<unsigned char *>(desc.get(2 * 16 * npos * nframes));
+        float *g = static_cast<float *>(gD.get(sizeof(float) * 16 * npos * nframes));
+        tr.get((size_t)prop_triplet_bytes() * batch);
+        float b1t = 1.0f, b2t = 1.0f;
+        for (int it = 0; it < iters; ++it) {
+            for (int k = 0; k < nframes; ++k)
+                CU(launch_prop_features(x.as<float>() + k * fs, W, W, H, wt.as<float>(), hid + 2 * 16 * px * k,
+                                        feat.get(2 * 16 * px), static_cast<float *>(rs.get(sizeof(float) * 16 * (size_t)H * (W - 3))),
+                                        dsc + 2 * 16 * npos * k, 0));
+            CU(launch_prop_sample(x.as<float>(), fs, W, W, H, nframes, lp.as<uint32_t>(), ln.as<int>(), G, dsy.as<int>(),
+                                  dsx.as<int>(), nby, nbx, R, (uint32_t)(seed * 1000003ull + (uint64_t)it), tr.p, batch, 0));
+            CU(cudaMemsetAsync(g, 0, sizeof(float) * 16 * npos * nframes, 0));
+            CU(cudaMemsetAsync(gw.get(sizeof(float) * kProposalWeightCount), 0, sizeof(float) * kProposalWeightCount, 0));
+            CU(launch_prop_loss(tr.p, batch, dsc, (long long)npos, Wd, g, 1.0f / batch, dl.as<float>() + it, 0));
+            for (int k = 0; k < nframes; ++k)
+                CU(launch_prop_backward(x.as<float>() + k * fs, W, W, H, wt.as<float>(), hid + 2 * 16 * px * k, g + 16 * npos * k,
+                                        static_cast<float *>(dF.get(sizeof(float) * 16 * px)),
+                                        static_cast<float *>(dH.get(sizeof(float) * 16 * px)), gw.as<float>(), 0));
+            b1t *= 0.9f;
+            b2t *= 0.999f;
+            CU(launch_prop_adam(wt.as<float>(), gw.as<float>(), mo.as<float>(), vo.as<float>(), lr, b1t, b2t, 0));
+        }
+        CU(cudaDeviceSynchronize());
+        CU(cudaMemcpy(weights, wt.p, sizeof(float) * kProposalWeightCount, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(losses, dl.p, sizeof(float) * iters, cudaMemcpyDeviceToHost));
+        return (int)BM3D_OK;
+    });
+}
+
+// Lists of one GRAY plane (block step `step`, group G, range R, candidate step 1, threshold
+// th_sse on the exact SSD): exhaustive when weights is null, else the learned proposals (the
+// best nprop candidates by descriptor distance, re-ranked exactly).  counts[nblocks], ys/xs
+// [nblocks][G]; returns the number of reference blocks.
+BM3D_API int bm3d_proposal_match(const float *frame, int width, int height, const float *weights, int step, int G, int R,
+                                 float th_sse, int nprop, int *counts, int *ys, int *xs, int capacity)
+{
+    g_error.clear();
+    if (!frame || !counts || !ys || !xs || width < 8 || height < 8 || G < 1 || G > 32 || R < 1 || step < 1 || nprop < 1 ||
+        nprop > 64)
+        return fail(BM3D_ERR_STATE, "bad arguments");
+    return guarded([&]() -> int {
+        const std::vector<int> syh = scan_positions(height, 8, step), sxh = scan_positions(width, 8, step);
+        const int nby = (int)syh.size(), nbx = (int)sxh.size(), nb = nby * nbx;
+        if (nb > capacity) throw std::runtime_error("capacity too small");
+        DevBuf x, wt, dsy, dsx, lp, ln;
+        PropBuffers pb;
+        CU(cudaMemcpy(x.get(sizeof(float) * width * height), frame, sizeof(float) * width * height, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(dsy.get(sizeof(int) * nby), syh.data(), sizeof(int) * nby, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(dsx.get(sizeof(int) * nbx), sxh.data(), sizeof(int) * nbx, cudaMemcpyHostToDevice));
+        const void *desc = nullptr;
+        if (weights) {
+            CU(cudaMemcpy(wt.get(sizeof(float) * kProposalWeightCount), weights, sizeof(float) * kProposalWeightCount, cudaMemcpyHostToDevice));
+            prop_descriptors(x.as<float>(), 0, width, width, height, 1, wt.as<float>(), pb, 0);
+            desc = pb.desc.p;
+        }
+        exhaustive_lists(x.as<float>(), 0, width, width, height, 1, step, G, R, th_sse, dsy.as<int>(), dsx.as<int>(), nby, nbx,
+                         static_cast<uint32_t *>(lp.get(sizeof(uint32_t) * nb * G)), static_cast<int *>(ln.get(sizeof(int) * nb)),
+                         desc, nprop, 0);
+        std::vector<uint32_t> P((size_t)nb * G);
+        CU(cudaDeviceSynchronize());
+        CU(cudaMemcpy(counts, ln.p, sizeof(int) * nb, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(P.data(), lp.p, sizeof(uint32_t) * P.size(), cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < P.size(); ++i) {
+            ys[i] = (int)unpack_y(P[i]);
+            xs[i] = (int)unpack_x(P[i]);
+        }
+        return nb;
+    });
 }
 
 BM3D_API int bm3d_debug_dct3d(float *groups, int ngroups, int n, int B, int inverse, int fast)

@@ -5,6 +5,7 @@
 #include "select.cuh"
 #include "bm.cuh"
 #include "bm_tc.cuh"
+#include "proposal.cuh"
 #include "vbm.cuh"
 #include "cf.cuh"
 #include "cf_tc.cuh"
@@ -46,6 +47,78 @@ cudaError_t launch_bm_tc(const BMArgs &a, const BmtLayout &L, int nframes, cudaS
     if ((e = allow_smem(bm_tc_kernel, smem)) != cudaSuccess) return e;
     COUNT_LAUNCH();
     bm_tc_kernel<<<grid, kBmtThreads, smem, s>>>(a, L);
+    return cudaGetLastError();
+}
+
+// ---- learned proposal ----------------------------------------------------------------------------
+
+int prop_triplet_bytes() { return (int)sizeof(PropTriplet); }
+
+cudaError_t launch_prop_features(const float *x, int ld, int W, int H, const float *wt, void *hid, void *feat, float *rs,
+                                 void *desc, cudaStream_t s)
+{
+    if (W < 8 || H < 8) return cudaErrorInvalidValue;
+    auto *h = static_cast<__nv_bfloat16 *>(hid);
+    auto *f = static_cast<__nv_bfloat16 *>(feat);
+    const dim3 blk(128);
+    COUNT_LAUNCH();
+    prop_conv1_kernel<<<dim3((W + 127) / 128, H), blk, 0, s>>>(x, ld, W, H, wt, h);
+    COUNT_LAUNCH();
+    prop_conv2_kernel<<<dim3((W + 127) / 128, H), blk, 0, s>>>(h, W, H, wt, f);
+    COUNT_LAUNCH();
+    prop_rowsum_kernel<<<dim3((W - 3 + 127) / 128, H, kPropCh), blk, 0, s>>>(f, W, H, rs);
+    COUNT_LAUNCH();
+    prop_desc_kernel<<<dim3((W - 7 + 127) / 128, H - 7), blk, 0, s>>>(rs, W, H, static_cast<__nv_bfloat16 *>(desc));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prop_loss(const void *triplets, int ntr, const void *desc, long long dstride, int Wd, float *gD,
+                             float scale, float *loss, cudaStream_t s)
+{
+    COUNT_LAUNCH();
+    prop_rank_loss_kernel<<<(ntr + 127) / 128, 128, 0, s>>>(static_cast<const PropTriplet *>(triplets), ntr,
+                                                           static_cast<const __nv_bfloat16 *>(desc), dstride, Wd, gD, scale, loss);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prop_backward(const float *x, int ld, int W, int H, const float *wt, const void *hid, const float *gD,
+                                 float *dF, float *dH, float *gw, cudaStream_t s)
+{
+    const dim3 blk(128), grd((W + 127) / 128, H);
+    COUNT_LAUNCH();
+    prop_desc_bwd_kernel<<<grd, blk, 0, s>>>(gD, W, H, dF);
+    COUNT_LAUNCH();
+    prop_conv2_bwd_kernel<<<grd, blk, 0, s>>>(static_cast<const __nv_bfloat16 *>(hid), dF, W, H, wt, gw, dH);
+    COUNT_LAUNCH();
+    prop_conv1_bwd_kernel<<<grd, blk, 0, s>>>(x, ld, dH, W, H, gw);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prop_adam(float *wt, const float *g, float *m, float *v, float lr, float b1t, float b2t, cudaStream_t s)
+{
+    COUNT_LAUNCH();
+    prop_adam_kernel<<<(kPropWeights + 255) / 256, 256, 0, s>>>(wt, g, m, v, lr, b1t, b2t);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prop_sample(const float *frames, long long fstride, int ld, int W, int H, int nframes, const uint32_t *lists,
+                               const int *counts, int G, const int *sy, const int *sx, int nby, int nbx, int range,
+                               uint32_t seed, void *out, int ntr, cudaStream_t s)
+{
+    COUNT_LAUNCH();
+    prop_sample_kernel<<<(ntr + 127) / 128, 128, 0, s>>>(frames, fstride, ld, W, H, nframes, lists, counts, G, sy, sx, nby,
+                                                        nbx, range, seed, static_cast<PropTriplet *>(out), ntr);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_bm_learned(const BMArgs &a, const void *desc, int nprop, int nframes, size_t smem, cudaStream_t s)
+{
+    if (a.B != 8 || a.G > 32) return cudaErrorInvalidValue;
+    dim3 grid((a.nbx + a.warps - 1) / a.warps, a.nby, nframes);
+    cudaError_t e;
+    if ((e = allow_smem(bm_learned_kernel, smem)) != cudaSuccess) return e;
+    COUNT_LAUNCH();
+    bm_learned_kernel<<<grid, 32 * a.warps, smem, s>>>(a, static_cast<const __nv_bfloat16 *>(desc), nprop);
     return cudaGetLastError();
 }
 

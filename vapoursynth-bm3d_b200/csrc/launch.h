@@ -12,6 +12,23 @@ namespace bm3d {
 cudaError_t upload_odd_tables(const float *host_odd_all);
 
 cudaError_t launch_bm_full(const BMArgs &a, int nframes, size_t smem_bytes, cudaStream_t s);
+// Learned proposal (no reference counterpart): feature network forward into bf16 hidden /
+// feature planes [16][H][W] (hid, feat), fp32 row sums rs [16][H][W - 7] and bf16 block descriptors
+// desc [H - 7][W - 7][16]; ranking loss, backward pass (dF, dH fp32 [16][H][W]; weight gradients
+// accumulated into gw), Adam, triplet sampling, and the matching kernel over descriptors.
+int prop_triplet_bytes();
+cudaError_t launch_prop_features(const float *x, int ld, int W, int H, const float *wt, void *hid, void *feat, float *rs,
+                                 void *desc, cudaStream_t s);
+cudaError_t launch_prop_loss(const void *triplets, int ntr, const void *desc, long long dstride, int Wd, float *gD,
+                             float scale, float *loss, cudaStream_t s);
+cudaError_t launch_prop_backward(const float *x, int ld, int W, int H, const float *wt, const void *hid, const float *gD,
+                                 float *dF, float *dH, float *gw, cudaStream_t s);
+cudaError_t launch_prop_adam(float *wt, const float *g, float *m, float *v, float lr, float b1t, float b2t, cudaStream_t s);
+cudaError_t launch_prop_sample(const float *frames, long long fstride, int ld, int W, int H, int nframes, const uint32_t *lists,
+                               const int *counts, int G, const int *sy, const int *sx, int nby, int nbx, int range,
+                               uint32_t seed, void *out, int ntr, cudaStream_t s);
+cudaError_t launch_bm_learned(const BMArgs &a, const void *desc, int nprop, int nframes, size_t smem, cudaStream_t s);
+
 // Precision-form full search (B = 8, candidate step 1, group size <= 32, search windows of
 // L.nrc consecutive reference blocks within 64 candidate columns): same lists as launch_bm_full.
 cudaError_t launch_bm_tc(const BMArgs &a, const BmtLayout &L, int nframes, cudaStream_t s);

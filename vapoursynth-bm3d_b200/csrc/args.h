@@ -29,6 +29,8 @@ BM3D_HD inline int bm_warp_floats(int cand_cap, int G, int B, bool generic)
 {
     return cand_cap + 64 + 2 * G + (generic ? B * B : 0);
 }
+// bm_learned_kernel: scores, then a 128-entry candidate list
+BM3D_HD inline int prop_warp_floats(int cand_cap) { return cand_cap + 128; }
 BM3D_HD inline int vbm_warp_floats(int sp_cap, int list_cap, int G, int ps_num, int B)
 {
     return 3 * sp_cap + 4 * list_cap + 2 * G + ps_num + B * B;

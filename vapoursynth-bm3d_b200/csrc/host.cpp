@@ -1053,14 +1053,15 @@ public:
         }
         if (warps < 1) throw std::runtime_error(err("bm_range / block_size too large for the shared-memory search window"));
         if (use_learned) {
-            // learned proposals: descriptors of every block position, then the best 2 G (at most
-            // 64) candidates by descriptor distance re-ranked with the exact SSD
+            // learned proposals: descriptors of every block position, then the best 64 candidates
+            // by descriptor distance re-ranked with the exact SSD
             if (!prop_wt.p) {
                 CU(cudaMemcpy(prop_wt.get(sizeof(float) * kProposalWeightCount), kProposalWeights,
                               sizeof(float) * kProposalWeightCount, cudaMemcpyHostToDevice));
             }
             prop_descriptors(a.ref, fs, ld, W, H, nout, prop_wt.as<float>(), prop_bufs, stream);
-            CU(launch_bm_learned(a, prop_bufs.desc.p, std::min(64, 2 * para.G), nout, smem, stream));
+            const size_t psmem = sizeof(float) * ((size_t)a.win_h * a.win_pitch + (size_t)a.warps * prop_warp_floats(a.cand_cap));
+            CU(launch_bm_learned(a, prop_bufs.desc.p, 64, nout, psmem, stream));
             return;
         }
         CU(launch_bm_full(a, nout, smem, stream));
@@ -1971,7 +1972,9 @@ static void exhaustive_lists(const float *planes, long long fs, int ld, int W, i
         if (smem <= 200 * 1024) break;
     }
     if (warps < 1) throw std::runtime_error("bm_range too large");
-    if (desc) CU(launch_bm_learned(a, desc, nprop, nframes, smem, stream));
+    if (desc) CU(launch_bm_learned(a, desc, nprop, nframes,
+                                   sizeof(float) * ((size_t)a.win_h * a.win_pitch + (size_t)a.warps * prop_warp_floats(a.cand_cap)),
+                                   stream));
     else CU(launch_bm_full(a, nframes, smem, stream));
 }
 

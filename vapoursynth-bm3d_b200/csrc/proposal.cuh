@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(256) bm_learned_kernel(BMArgs a, const __nv_bf
     __syncthreads();
     if (bx >= a.nbx) return;
 
-    float *sd = smem + a.win_h * wp + warp * bm_warp_floats(a.cand_cap, a.G, 8, false);
+    float *sd = smem + a.win_h * wp + warp * prop_warp_floats(a.cand_cap);
     uint32_t *list = reinterpret_cast<uint32_t *>(sd + a.cand_cap);
     const int i = a.scan_x[bx];
     const size_t ob = ((size_t)f * a.nby + by) * a.nbx + bx;
@@ -381,30 +381,51 @@ __global__ void __launch_bounds__(256) bm_learned_kernel(BMArgs a, const __nv_bf
         sd[c] = (c < clat && cy == j && cx == i) ? 3.0e38f : sc;
     }
     __syncwarp();
-    // the nprop best scores: two per lane, a 64-entry sort, then everything at or below the cut
-    uint64_t b1 = ~0ull, b2 = ~0ull;
+    // the nprop best scores: four per lane, a 128-entry sort gives a cut at or above the true
+    // nprop-th score; every candidate at or below it (at most 128 kept) sorted, the first nprop
+    uint64_t bb[4] = {~0ull, ~0ull, ~0ull, ~0ull};
     for (int c0 = 0; c0 < ctot; c0 += 32) {
         const int c = c0 + ((lane + 7 * (c0 >> 5)) & 31);
         if (c >= ctot) continue;
-        const uint64_t v = compose(sd[c], (uint32_t)c);
-        if (v < b1) { b2 = b1; b1 = v; } else if (v < b2) { b2 = v; }
+        uint64_t v = compose(sd[c], (uint32_t)c);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint64_t lo = v < bb[e] ? v : bb[e];
+            v = v < bb[e] ? bb[e] : v;
+            bb[e] = lo;
+        }
     }
-    uint64_t v2[2] = {b1, b2};
-    warp_bitonic_u64<2>(v2);
+    warp_bitonic_u64<4>(bb);
     const int pr = min(nprop, 64) - 1;                  // rank of the last proposal
-    const uint64_t c0v = __shfl_sync(0xffffffffu, v2[0], pr & 31), c1v = __shfl_sync(0xffffffffu, v2[1], pr & 31);
-    const uint64_t cut = pr < 32 ? c0v : c1v;
+    uint64_t cv[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) cv[e] = __shfl_sync(0xffffffffu, bb[e], pr & 31);
+    const uint64_t cut = cv[pr >> 5];
     const unsigned lt = (1u << lane) - 1u;
     int m = 0;
     for (int c0 = 0; c0 < ctot; c0 += 32) {
         const int c = c0 + lane;
         const bool in = c < ctot && compose(sd[c], (uint32_t)c) <= cut;
         const unsigned msk = __ballot_sync(0xffffffffu, in);
-        if (in && m + __popc(msk & lt) < 64) list[m + __popc(msk & lt)] = (uint32_t)c;
+        if (in && m + __popc(msk & lt) < 128) list[m + __popc(msk & lt)] = (uint32_t)c;
         m += __popc(msk);
     }
     __syncwarp();
-    m = min(m, 64);
+    m = min(m, 128);
+    if (m > pr + 1) {
+        uint64_t sv[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int idx = lane + 32 * e;
+            sv[e] = idx < m ? compose(sd[list[idx]], list[idx]) : ~0ull;
+        }
+        warp_bitonic_u64<4>(sv);
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < 2; ++e) list[lane + 32 * e] = (uint32_t)sv[e];
+        __syncwarp();
+        m = pr + 1;
+    }
     // exact distances of the proposals, valid ones ordered by (key, scan index)
     const float *rp = win + (j - wy0) * wp + (i - wx0);
     uint64_t v[2] = {~0ull, ~0ull};

@@ -83,8 +83,11 @@ struct TcShape {
     // a reference box and the aggregation box, so that the next plane's boxes load while this
     // plane is filtered; otherwise one box serves the gathers and the aggregation in turn.
     static constexpr int kBoxes = WIENER && kZInTmem ? 3 : 1;
-    static constexpr int kRegion = kBoxes == 3 ? 2688 : 3072;   // floats per box
-    static constexpr int kExtra = kPart + kRegion * 4 * kBoxes + 256;   // + 2 x [4 quarters][8] ints of scratch
+    static constexpr int kRegion = kBoxes == 3 ? 2560 : 3072;   // floats per box
+    // three-box form: a table of the tile's rows (block position in the box, weight) that the
+    // block-step loops read with one broadcast load instead of three or four shuffles
+    static constexpr int kRowTab = kBoxes == 3 ? 128 * 8 : 0;
+    static constexpr int kExtra = kPart + kRegion * 4 * kBoxes + 256 + kRowTab;   // + 2 x [4 quarters][8] ints of scratch
     static constexpr int kSmem = (kData + kExtra) * kWG + TcLayout<G>::kTableBytes - kTabOff;
 };
 
@@ -130,6 +133,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     float *Br = Shp::kBoxes == 3 ? Rg + 2 * Shp::kRegion : Rg;          // reference box
     int *bbx = reinterpret_cast<int *>(extra + Shp::kPart + Shp::kRegion * 4 * Shp::kBoxes);   // [4 quarters][8]: maxima
     int *bnd = bbx + 32;                                                  // [4 quarters][8]: tile bounds
+    // [128]: (y - y0) << 16 | (x - x0) of the row's block in the box (-1: not this kernel's), numW bits
+    int2 *rowtab = reinterpret_cast<int2 *>(extra + Shp::kPart + Shp::kRegion * 4 * Shp::kBoxes + 256);
     // table byte b lives at tab + b (b >= kTabOff)
     unsigned char *tab = tsm + (Shp::kData + Shp::kExtra) * NWG - Shp::kTabOff;
 
@@ -354,12 +359,14 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             // 1. gather (rows of foreign or partial groups are zero), one block per warp step
             if (region) {
                 if constexpr (Shp::kBoxes == 3) {
+                    if (half == 0) rowtab[r].x = mine ? ((L.y - y0) << 16) | (L.x - x0) : -1;
                     tc::cp_async_wait_all();
                     tc::wg_sync(bar_id, TEAM);
 #pragma unroll 4
                     for (int i = half * NI; i < half * NI + NI; ++i) {
-                        const bool mi = __shfl_sync(0xffffffffu, mine, i);
-                        const int by = __shfl_sync(0xffffffffu, L.y, i) - y0, bx = __shfl_sync(0xffffffffu, L.x, i) - x0;
+                        const int pq = rowtab[b0 + i].x;
+                        const bool mi = pq >= 0;
+                        const int by = pq >> 16, bx = pq & 0xffff;
                         float v0 = 0.f, v1 = 0.f, u0 = 0.f, u1 = 0.f;
                         if (mi) {
                             v0 = Bs[(by + ry) * rp + bx + cx];
@@ -540,6 +547,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) cmax = fmaxf(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
                 if ((t & 31) == 0) reinterpret_cast<float *>(bbx)[t >> 5] = cmax;
+                if constexpr (Shp::kBoxes == 3)
+                    if (half == 0) rowtab[r].y = __float_as_int(numW);
                 int *Ri = reinterpret_cast<int *>(Rg);
                 if (Shp::kBoxes == 1 && region)           // (the three-box form clears it in the flush)
                     for (int e = t; e < rh * rp; e += TEAM) Ri[e] = 0;
@@ -559,6 +568,18 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 float *np = L.num + (long long)L.y * a.ld + L.x;
 #pragma unroll 4
                 for (int i = half * NI; i < half * NI + NI; ++i) {
+                    if (Shp::kBoxes == 3 && region) {
+                        const int2 q = rowtab[b0 + i];
+                        if (q.x >= 0) {
+                            const int by = q.x >> 16, bx = q.x & 0xffff;
+                            const float ws = __int_as_float(q.y) * scale;
+                            const float x0v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane, 128));
+                            const float x1v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128));
+                            atomicAdd(Ri + (by + ry) * rp + bx + cx, __float2int_rn(x0v * ws));
+                            atomicAdd(Ri + (by + ry + 4) * rp + bx + cx, __float2int_rn(x1v * ws));
+                        }
+                        continue;
+                    }
                     const bool mi = __shfl_sync(0xffffffffu, mine, i);
                     const float wi = __shfl_sync(0xffffffffu, numW, i);
                     if (region) {

@@ -130,6 +130,10 @@ struct CFArgs {
     float *scratch;            // per-warp scratch for the generic path
     long long scratch_per_warp;
     int skip_full;             // generic kernel: skip groups the fast kernel handles
+    // optional (fast kernel with skip_full): the partial groups' indices and their count on the
+    // device; the kernel then walks this list instead of every group
+    const long long *plist;
+    const unsigned int *plist_n;
 };
 
 struct VBMArgs {

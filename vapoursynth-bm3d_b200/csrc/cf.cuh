@@ -243,6 +243,24 @@ __device__ __forceinline__ const float *dtab_for(const CFArgs &a, int N, bool in
     return off < 0 ? nullptr : a.dtab + off + (inverse ? N * N : 0);
 }
 
+// Indices of the groups with fewer than G blocks (the ones the tensor-core filter leaves), in any
+// order (their aggregation is order-free atomics): one warp-aggregated atomic per warp step.
+__global__ void cf_partial_list_kernel(const int *__restrict__ count, long long ngroups, int G, long long *__restrict__ list,
+                                       unsigned int *__restrict__ n)
+{
+    const int lane = (int)lane_id();
+    for (long long g0 = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); g0 < ngroups;
+         g0 += (long long)gridDim.x * blockDim.x) {
+        const long long g = g0 + lane;
+        const bool part = g < ngroups && count[g] < G;
+        const unsigned m = __ballot_sync(0xffffffffu, part);
+        unsigned base = 0;
+        if (lane == 0 && m) base = atomicAdd(n, (unsigned)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (part) list[base + __popc(m & ((1u << lane) - 1u))] = g;
+    }
+}
+
 // The collaborative-filter kernel: per-lane gathers straight into registers, register-resident
 // 2-D transforms, the z stage inline for full groups (out-of-line calls only for the rare partial
 // groups), and per-lane global float atomics into the numerator and per-origin weight planes.
@@ -273,9 +291,12 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
     float *T2 = T + 32 * kTP;
 
     const long long nwarps = (long long)gridDim.x * nwarp;
-    for (long long wg = (long long)blockIdx.x * nwarp + warp; wg * GPW < a.ngroups; wg += nwarps) {
-        const long long grp = wg * GPW + sub;
-        const bool inrange = grp < a.ngroups;
+    // with a partial-group list the warps walk the list (one group per slot), else every group
+    const long long nitems = a.plist ? (long long)*a.plist_n : a.ngroups;
+    for (long long wg = (long long)blockIdx.x * nwarp + warp; wg * GPW < nitems; wg += nwarps) {
+        const long long item = wg * GPW + sub;
+        const bool inrange = item < nitems;
+        const long long grp = a.plist ? (inrange ? a.plist[item] : 0) : item;
         const long long g0 = inrange ? grp : 0;
         const int n = min(a.count[g0], G);
         // skip_full: full groups were filtered by the tensor-core kernel; only partial ones here

@@ -894,7 +894,7 @@ public:
     DevBuf m_pos, m_n, m_key, v_pos, v_n, v_key;
     DevBuf d_sy, d_sx, scratch;
     DevBuf d_winb, d_winl, d_winc, d_slot0;
-    DevBuf tc_tab, tc_status;
+    DevBuf tc_tab, tc_status, plist, plist_n;
     DirectTables dtabs;
     int last_count = 0;
 
@@ -1111,6 +1111,13 @@ public:
             // precision form: full groups on the tensor cores, partial ones on the plain kernel
             CU(launch_cf_tc(a, tc_tab.p, tc_status.as<int>(), stream));
             a.skip_full = 1;
+            // the plain kernel walks a list of the partial groups instead of skipping the full ones
+            long long *pl = static_cast<long long *>(plist.get(sizeof(long long) * (size_t)std::max<long long>(1, ngroups)));
+            unsigned int *pn = static_cast<unsigned int *>(plist_n.get(sizeof(unsigned int)));
+            CU(cudaMemsetAsync(pn, 0, sizeof(unsigned int), stream));
+            CU(launch_cf_partial_list(cnt, ngroups, para.G, pl, pn, stream));
+            a.plist = pl;
+            a.plist_n = pn;
         }
         if (fast) CU(launch_cf_fast(a, stream));
         if (!fast) {

@@ -178,6 +178,14 @@ static cudaError_t launch_cf_fast_t(const CFArgs &a, cudaStream_t s)
     return cudaGetLastError();
 }
 
+cudaError_t launch_cf_partial_list(const int *count, long long ngroups, int G, long long *list, unsigned int *n, cudaStream_t s)
+{
+    const long long blocks = std::max<long long>(1, std::min<long long>((ngroups + 255) / 256, 148LL * 16));
+    COUNT_LAUNCH();
+    cf_partial_list_kernel<<<(unsigned)blocks, 256, 0, s>>>(count, ngroups, G, list, n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_cf_fast(const CFArgs &a, cudaStream_t s)
 {
     if (a.B != 8) return cudaErrorInvalidValue;

@@ -36,6 +36,8 @@ cudaError_t launch_vbm_predict(const VBMArgs &a, int nframes, size_t smem_bytes,
 // Fast collaborative filter (B = 8, G in {8, 16, 32}, any group length n <= G); sizes its own
 // grid (one CTA per run of consecutive groups); returns cudaErrorInvalidValue for other shapes.
 cudaError_t launch_cf_fast(const CFArgs &a, cudaStream_t s);
+// Indices of the groups with count < G into list (device counter n, zeroed by the caller).
+cudaError_t launch_cf_partial_list(const int *count, long long ngroups, int G, long long *list, unsigned int *n, cudaStream_t s);
 cudaError_t launch_cf_generic(const CFArgs &a, int warps, int grid, cudaStream_t s);
 cudaError_t launch_convert(const ConvProgram &pr, const PlanePtr *in_dev, const PlanePtr *out_dev,
                            int nframes, cudaStream_t s);

@@ -216,7 +216,7 @@ BM3D_API int bm3d_proposal_gradients(const float *frame, int width, int height, 
 BM3D_API int bm3d_proposal_train(const float *frames, int nframes, int width, int height, int iters, int batch, float lr,
                                  uint64_t seed, float *weights, float *losses);
 /* Match lists of one plane (block step, group size <= 32, range, candidate step 1, SSD threshold):
- * exhaustive when weights is NULL, else the nprop (<= 64) best candidates by descriptor distance
+ * exhaustive when weights is NULL, else the nprop (<= 128) best candidates by descriptor distance
  * re-ranked with the exact SSD.  counts[n], ys / xs [n][group_size]; capacity = room for n. */
 BM3D_API int bm3d_proposal_match(const float *frame, int width, int height, const float *weights, int block_step,
                                  int group_size, int bm_range, float th_sse, int nprop, int *counts, int *ys, int *xs,

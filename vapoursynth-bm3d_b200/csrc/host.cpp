@@ -700,6 +700,9 @@ public:
 // ---------------------------------------------------------------------------------------------
 // Learned block-matching proposal: device buffers and the descriptor pass
 
+// proposals per reference block that the learned form re-ranks exactly (of about 1,089 at range 16)
+constexpr int kLearnedProposals = 96;
+
 struct PropBuffers {
     DevBuf hid, feat, rs, desc, grad_d, dF, dH;
 };
@@ -1053,15 +1056,15 @@ public:
         }
         if (warps < 1) throw std::runtime_error(err("bm_range / block_size too large for the shared-memory search window"));
         if (use_learned) {
-            // learned proposals: descriptors of every block position, then the best 64 candidates
-            // by descriptor distance re-ranked with the exact SSD
+            // learned proposals: descriptors of every block position, then the best
+            // kLearnedProposals candidates by descriptor distance re-ranked with the exact SSD
             if (!prop_wt.p) {
                 CU(cudaMemcpy(prop_wt.get(sizeof(float) * kProposalWeightCount), kProposalWeights,
                               sizeof(float) * kProposalWeightCount, cudaMemcpyHostToDevice));
             }
             prop_descriptors(a.ref, fs, ld, W, H, nout, prop_wt.as<float>(), prop_bufs, stream);
             const size_t psmem = sizeof(float) * ((size_t)a.win_h * a.win_pitch + (size_t)a.warps * prop_warp_floats(a.cand_cap));
-            CU(launch_bm_learned(a, prop_bufs.desc.p, 64, nout, psmem, stream));
+            CU(launch_bm_learned(a, prop_bufs.desc.p, kLearnedProposals, nout, psmem, stream));
             return;
         }
         CU(launch_bm_full(a, nout, smem, stream));
@@ -2120,7 +2123,7 @@ BM3D_API int bm3d_proposal_match(const float *frame, int width, int height, cons
 {
     g_error.clear();
     if (!frame || !counts || !ys || !xs || width < 8 || height < 8 || G < 1 || G > 32 || R < 1 || step < 1 || nprop < 1 ||
-        nprop > 64)
+        nprop > 128)
         return fail(BM3D_ERR_STATE, "bad arguments");
     return guarded([&]() -> int {
         const std::vector<int> syh = scan_positions(height, 8, step), sxh = scan_positions(width, 8, step);

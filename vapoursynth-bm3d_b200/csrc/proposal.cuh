@@ -381,8 +381,8 @@ __global__ void __launch_bounds__(256) bm_learned_kernel(BMArgs a, const __nv_bf
         sd[c] = (c < clat && cy == j && cx == i) ? 3.0e38f : sc;
     }
     __syncwarp();
-    // the nprop best scores: four per lane, a 128-entry sort gives a cut at or above the true
-    // nprop-th score; every candidate at or below it (at most 128 kept) sorted, the first nprop
+    // the nprop (<= 128) best scores: four per lane, a 128-entry sort gives a cut at or above the
+    // true nprop-th score; every candidate at or below it (at most 128 kept) sorted, the first nprop
     uint64_t bb[4] = {~0ull, ~0ull, ~0ull, ~0ull};
     for (int c0 = 0; c0 < ctot; c0 += 32) {
         const int c = c0 + ((lane + 7 * (c0 >> 5)) & 31);
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(256) bm_learned_kernel(BMArgs a, const __nv_bf
         }
     }
     warp_bitonic_u64<4>(bb);
-    const int pr = min(nprop, 64) - 1;                  // rank of the last proposal
+    const int pr = min(nprop, 128) - 1;                 // rank of the last proposal
     uint64_t cv[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) cv[e] = __shfl_sync(0xffffffffu, bb[e], pr & 31);
@@ -422,16 +422,16 @@ __global__ void __launch_bounds__(256) bm_learned_kernel(BMArgs a, const __nv_bf
         warp_bitonic_u64<4>(sv);
         __syncwarp();
 #pragma unroll
-        for (int e = 0; e < 2; ++e) list[lane + 32 * e] = (uint32_t)sv[e];
+        for (int e = 0; e < 4; ++e) list[lane + 32 * e] = (uint32_t)sv[e];
         __syncwarp();
         m = pr + 1;
     }
     // exact distances of the proposals, valid ones ordered by (key, scan index)
     const float *rp = win + (j - wy0) * wp + (i - wx0);
-    uint64_t v[2] = {~0ull, ~0ull};
+    uint64_t v[4] = {~0ull, ~0ull, ~0ull, ~0ull};
     int nval = 0;
 #pragma unroll
-    for (int e = 0; e < 2; ++e) {
+    for (int e = 0; e < 4; ++e) {
         const int idx = lane + 32 * e;
         if (idx < m) {
             const uint32_t c = list[idx];
@@ -449,7 +449,8 @@ __global__ void __launch_bounds__(256) bm_learned_kernel(BMArgs a, const __nv_bf
         }
     }
     nval = warp_sum(nval);
-    warp_bitonic_u64<2>(v);
+    if (m <= 64) warp_bitonic_u64<2>(*reinterpret_cast<uint64_t (*)[2]>(v));
+    else warp_bitonic_u64<4>(v);
     const int nout = min(nval, K);
     if (lane < nout) {
         const uint32_t c = (uint32_t)v[0];

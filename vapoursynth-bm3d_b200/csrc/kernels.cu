@@ -64,7 +64,7 @@ cudaError_t launch_prop_features(const float *x, int ld, int W, int H, const flo
     COUNT_LAUNCH();
     prop_conv1_kernel<<<dim3((W + 127) / 128, H), blk, 0, s>>>(x, ld, W, H, wt, h);
     COUNT_LAUNCH();
-    prop_conv2_kernel<<<dim3((W + 127) / 128, H), blk, 0, s>>>(h, W, H, wt, f);
+    prop_conv2_kernel<<<dim3((W + 128 * kPropConv2Px - 1) / (128 * kPropConv2Px), H), blk, 0, s>>>(h, W, H, wt, f);
     COUNT_LAUNCH();
     prop_rowsum_kernel<<<dim3((W - 3 + 127) / 128, H, kPropCh), blk, 0, s>>>(f, W, H, rs);
     COUNT_LAUNCH();

@@ -54,32 +54,48 @@ __global__ void prop_conv1_kernel(const float *__restrict__ x, int ld, int W, in
     }
 }
 
-// F[c][y][x] = b2[c] + sum_{i,k} w2[c][i][k] H[i](y + dy, x + dx), bf16 planar [16][H][W]
+// F[c][y][x] = b2[c] + sum_{i,k} w2[c][i][k] H[i](y + dy, x + dx), bf16 planar [16][H][W].  Each
+// thread computes 4 consecutive pixels, so every weight read from shared memory serves 4 products
+// (the sum order per output is the same as one pixel per thread: i outer, tap k inner).
+constexpr int kPropConv2Px = 4;
 __global__ void prop_conv2_kernel(const __nv_bfloat16 *__restrict__ hid, int W, int H, const float *__restrict__ wt,
                                   __nv_bfloat16 *__restrict__ feat)
 {
     __shared__ float w[kPropCh * kPropCh * 9 + kPropCh];
     for (int i = threadIdx.x; i < kPropCh * kPropCh * 9 + kPropCh; i += blockDim.x) w[i] = wt[kPropW2 + i];
     __syncthreads();
-    const int px = blockIdx.x * blockDim.x + threadIdx.x, py = blockIdx.y;
-    if (px >= W) return;
-    float acc[kPropCh];
+    const int px0 = (blockIdx.x * blockDim.x + threadIdx.x) * kPropConv2Px, py = blockIdx.y;
+    if (px0 >= W) return;
+    float acc[kPropConv2Px][kPropCh];
 #pragma unroll
-    for (int c = 0; c < kPropCh; ++c) acc[c] = w[kPropCh * kPropCh * 9 + c];
+    for (int q = 0; q < kPropConv2Px; ++q)
+#pragma unroll
+        for (int c = 0; c < kPropCh; ++c) acc[q][c] = w[kPropCh * kPropCh * 9 + c];
     for (int i = 0; i < kPropCh; ++i) {
-        float v[9];
+        float v[3][kPropConv2Px + 2];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const int yy = py + k / 3 - 1, xx = px + k % 3 - 1;
-            v[k] = (yy >= 0 && yy < H && xx >= 0 && xx < W) ? __bfloat162float(hid[((long long)i * H + yy) * W + xx]) : 0.0f;
+        for (int dy = 0; dy < 3; ++dy) {
+            const int yy = py + dy - 1;
+#pragma unroll
+            for (int u = 0; u < kPropConv2Px + 2; ++u) {
+                const int xx = px0 + u - 1;
+                v[dy][u] = (yy >= 0 && yy < H && xx >= 0 && xx < W) ? __bfloat162float(hid[((long long)i * H + yy) * W + xx]) : 0.0f;
+            }
         }
 #pragma unroll
-        for (int c = 0; c < kPropCh; ++c)
+        for (int k = 0; k < 9; ++k)
 #pragma unroll
-            for (int k = 0; k < 9; ++k) acc[c] = fmaf(w[(c * kPropCh + i) * 9 + k], v[k], acc[c]);
+            for (int c = 0; c < kPropCh; ++c) {
+                const float wv = w[(c * kPropCh + i) * 9 + k];
+#pragma unroll
+                for (int q = 0; q < kPropConv2Px; ++q) acc[q][c] = fmaf(wv, v[k / 3][q + k % 3], acc[q][c]);
+            }
     }
 #pragma unroll
-    for (int c = 0; c < kPropCh; ++c) feat[((long long)c * H + py) * W + px] = __float2bfloat16_rn(acc[c]);
+    for (int q = 0; q < kPropConv2Px; ++q)
+        if (px0 + q < W)
+#pragma unroll
+            for (int c = 0; c < kPropCh; ++c) feat[((long long)c * H + py) * W + px0 + q] = __float2bfloat16_rn(acc[q][c]);
 }
 
 // Block descriptors: D[y][x][c] = mean of F[c] over the 4x4 quadrant q = c % 4 (rows 4 (q / 2) ..,

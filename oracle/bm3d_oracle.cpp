@@ -456,6 +456,60 @@ static void dct3d(float *g, int n, int B, bool inverse)
 }
 
 // ---------------------------------------------------------------------------------------------
+// Statistics for the parity reports (no reference counterpart; they only observe the arithmetic)
+
+struct Stats {
+    std::atomic<long long> groups{0};       // groups filtered (per plane)
+    std::atomic<long long> coefs{0};        // hard-threshold decisions taken
+    std::atomic<long long> flips{0};        // decisions that differ from the FP64 evaluation
+    std::atomic<long long> band{0};         // |c| within a relative 2^-10 of its threshold
+    std::atomic<long long> blocks{0};       // reference blocks matched
+    std::atomic<long long> tie_blocks{0};   // blocks with equal keys inside the kept list or at its cut
+};
+
+// FP64 forward 3-D DCT of one group by the REDFT10 definition (Y_k = 2 sum_j x_j cos(pi (j+1/2)
+// k / N)) along x, y, then z.  Used only to count threshold decisions that FP32 rounding flips.
+static void dct3d_f64(std::vector<double> &g, int n, int B)
+{
+    const ptrdiff_t plane = (ptrdiff_t)B * B;
+    static std::once_flag once[257];
+    static std::vector<double> cosk[257];      // [k][j] = 2 cos(pi (j + 1/2) k / N)
+    auto table = [](int N) -> const double * {
+        std::call_once(once[N], [N]() {
+            cosk[N].resize((size_t)N * N);
+            for (int k = 0; k < N; ++k)
+                for (int j = 0; j < N; ++j) cosk[N][(size_t)k * N + j] = 2.0 * std::cos(M_PI * (j + 0.5) * k / N);
+        });
+        return cosk[N].data();
+    };
+    auto line = [&](double *d, int N, ptrdiff_t stride) {
+        const double *c = table(N);
+        double in[256], out[256];
+        for (int j = 0; j < N; ++j) in[j] = d[j * stride];
+        for (int k = 0; k < N; ++k) {
+            double acc = 0;
+            for (int j = 0; j < N; ++j) acc += in[j] * c[(size_t)k * N + j];
+            out[k] = acc;
+        }
+        for (int k = 0; k < N; ++k) d[k * stride] = out[k];
+    };
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < B; ++y) line(g.data() + z * plane + y * B, B, 1);
+    for (int z = 0; z < n; ++z)
+        for (int x = 0; x < B; ++x) line(g.data() + z * plane + x, B, B);
+    for (ptrdiff_t q = 0; q < plane; ++q) line(g.data() + q, n, plane);
+}
+
+// Tie events of a selected list (include/Block.h:715-728): equal keys among the kept entries
+// after the pinned first one, or between the last kept entry and the best one dropped.
+static bool has_tie(const std::vector<float> &kept, float best_dropped, bool dropped_any, int first)
+{
+    for (size_t k = first; k + 1 < kept.size(); ++k)
+        if (kept[k] == kept[k + 1]) return true;
+    return dropped_any && !kept.empty() && kept.back() == best_dropped;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Block matching (include/Block.h:554-827)
 
 struct Pos {
@@ -566,7 +620,7 @@ static void load_block(const float *plane, ptrdiff_t stride, int j, int i, int B
 // stable_sort otherwise.
 static std::vector<Match> bm_range(const float *plane, int H, int W, ptrdiff_t stride,
                                    int j, int i, int B, int range, int step, double thMSE,
-                                   int match_size, int z = 0)
+                                   int match_size, int z = 0, bool *ties = nullptr)
 {
     range = range / step * step;
     const int l = search_boundary(i, 0, range, step);
@@ -590,9 +644,21 @@ static std::vector<Match> bm_range(const float *plane, int H, int W, ptrdiff_t s
     bm_core(code, blk, B, plane, stride, sp, bm_const(B, thMSE), z);
     if (match_size > 0 && code.size() > (size_t)match_size) {
         std::partial_sort(code.begin() + 1, code.begin() + match_size, code.end());
+        if (ties) {
+            float best = std::numeric_limits<float>::infinity();
+            for (size_t k = match_size; k < code.size(); ++k) best = std::min(best, code[k].key);
+            std::vector<float> kept;
+            for (int k = 0; k < match_size; ++k) kept.push_back(code[k].key);
+            *ties = has_tie(kept, best, true, 1);
+        }
         code.resize(match_size);
     } else {
         std::stable_sort(code.begin(), code.end());
+        if (ties) {
+            std::vector<float> kept;
+            for (const Match &m : code) kept.push_back(m.key);
+            *ties = has_tie(kept, 0.0f, false, 1);
+        }
     }
     return code;
 }
@@ -676,50 +742,69 @@ static void gather(float *g, const std::vector<Match> &code, int n, int B,
     }
 }
 
-struct CFStats {
-    long long groups = 0;
-};
-
-static void cf_basic(const PlaneData &pd, int G, int B, const std::vector<Match> &code,
-                     const float *const *src, ptrdiff_t stride, const Accum &acc,
-                     std::vector<float> &buf)
+// Hard threshold of one group (source/BM3D_Basic.cpp:72-148) up to the scatter: gather, forward
+// 3-D DCT, keep c iff |c| > thr, count the retained coefficients, inverse DCT.  The filtered
+// group is left in g; numW / denW are the aggregation weights.  With st, the threshold decisions
+// are also taken on an FP64 evaluation of the transform and the disagreements counted.
+static int cf_basic_filter(const PlaneData &pd, int G, int B, const std::vector<Match> &code,
+                           const float *const *src, ptrdiff_t stride, std::vector<float> &g,
+                           float &numW, float &denW, Stats *st)
 {
     int n = (int)code.size();
     if (G > 0 && n > G) n = G;
     const size_t sz = (size_t)n * B * B;
-    buf.resize(sz);
-    float *g = buf.data();
-    gather(g, code, n, B, src, stride);
-    dct3d(g, n, B, false);
+    g.resize(sz);
+    gather(g.data(), code, n, B, src, stride);
+    std::vector<double> g64;
+    if (st) {
+        g64.assign(g.begin(), g.end());
+        dct3d_f64(g64, n, B);
+    }
+    dct3d(g.data(), n, B, false);
     const float *thr = pd.thr[n - 1].data();
     int retained = 0;
+    long long flips = 0, band = 0;
     for (size_t q = 0; q < sz; ++q) {
-        if (std::fabs(g[q]) > thr[q]) ++retained;
+        const bool keep = std::fabs(g[q]) > thr[q];
+        if (st) {
+            flips += keep != (std::fabs(g64[q]) > (double)thr[q]);
+            band += std::fabs(std::fabs(g[q]) - thr[q]) <= thr[q] * (1.0f / 1024.0f);
+        }
+        if (keep) ++retained;
         else g[q] = 0.0f;
     }
-    dct3d(g, n, B, true);
-    float denW = retained < 1 ? 1.0f : 1.0f / static_cast<float>(retained);
-    float numW = static_cast<float>(denW / pd.finalAMP[n - 1]);
-    scatter(g, code, n, B, acc, numW, denW);
+    if (st) {
+        st->groups += 1;
+        st->coefs += (long long)sz;
+        st->flips += flips;
+        st->band += band;
+    }
+    dct3d(g.data(), n, B, true);
+    denW = retained < 1 ? 1.0f : 1.0f / static_cast<float>(retained);
+    numW = static_cast<float>(denW / pd.finalAMP[n - 1]);
+    return n;
 }
 
 // wiener_mode 0: exact division with a sequential L2 sum (the reference's non-SSE build,
 // source/BM3D_Final.cpp:106-112); 1: the x86 SSE build (source/BM3D_Final.cpp:78-104):
-// four-lane L2 partial sums and an approximate reciprocal from _mm_rcp_ps.
-static void cf_final(const PlaneData &pd, int G, int B, const std::vector<Match> &code,
-                     const float *const *src, const float *const *ref, ptrdiff_t stride,
-                     const Accum &acc, std::vector<float> &buf, int wiener_mode)
+// four-lane L2 partial sums and an approximate reciprocal from _mm_rcp_ps.  rg is scratch.
+static int cf_final_filter(const PlaneData &pd, int G, int B, const std::vector<Match> &code,
+                           const float *const *src, const float *const *ref, ptrdiff_t stride,
+                           std::vector<float> &gv, std::vector<float> &rgv, int wiener_mode,
+                           float &numW, float &denW, Stats *st)
 {
     int n = (int)code.size();
     if (G > 0 && n > G) n = G;
     const size_t sz = (size_t)n * B * B;
-    buf.resize(2 * sz);
-    float *g = buf.data();
-    float *rg = g + sz;
+    gv.resize(sz);
+    rgv.resize(sz);
+    float *g = gv.data();
+    float *rg = rgv.data();
     gather(g, code, n, B, src, stride);
     gather(rg, code, n, B, ref, stride);
     dct3d(g, n, B, false);
     dct3d(rg, n, B, false);
+    if (st) st->groups += 1;
     const float sig2 = pd.wsig2[n - 1];
     float L2 = 0;
     size_t q = 0;
@@ -750,9 +835,31 @@ static void cf_final(const PlaneData &pd, int G, int B, const std::vector<Match>
     dct3d(g, n, B, true);
     const float eps = std::numeric_limits<float>::epsilon();
     L2 = L2 > eps ? L2 : eps;
-    float denW = 1.0f / L2;
-    float numW = static_cast<float>(denW / pd.finalAMP[n - 1]);
-    scatter(g, code, n, B, acc, numW, denW);
+    denW = 1.0f / L2;
+    numW = static_cast<float>(denW / pd.finalAMP[n - 1]);
+    return n;
+}
+
+// Runs f(i, worker) for i in [0, n) on `workers` threads (the caller's thread is worker 0).
+template <class F>
+static void parallel_for(int n, int workers, F &&f)
+{
+    if (workers <= 1 || n < 2) {
+        for (int i = 0; i < n; ++i) f(i, 0);
+        return;
+    }
+    std::atomic<int> next(0);
+    auto run = [&](int w) {
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= n) break;
+            f(i, w);
+        }
+    };
+    std::vector<std::thread> th;
+    for (int w = 1; w < workers; ++w) th.emplace_back(run, w);
+    run(0);
+    for (auto &t : th) t.join();
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -779,16 +886,78 @@ static void scan_positions(int extent, int B, int step, std::vector<int> &out)
 
 // BlockMatching wrapper (source/BM3D_Base.cpp:473-490)
 static std::vector<Match> bm3d_match(const Para &p, const float *refY, int H, int W,
-                                     ptrdiff_t stride, int j, int i)
+                                     ptrdiff_t stride, int j, int i, Stats *st = nullptr)
 {
     if (p.G == 1 || p.thMSE <= 0) return std::vector<Match>(1, Match{0.0f, 0, j, i});
-    return bm_range(refY, H, W, stride, j, i, p.B, p.R, p.bmstep, p.thMSE, p.G);
+    bool ties = false;
+    std::vector<Match> code = bm_range(refY, H, W, stride, j, i, p.B, p.R, p.bmstep, p.thMSE, p.G, 0,
+                                       st ? &ties : nullptr);
+    if (st) {
+        st->blocks += 1;
+        st->tie_blocks += ties;
+    }
+    return code;
+}
+
+// One reference block's filtered groups for every processed plane, ready to scatter.
+struct BlockOut {
+    std::vector<Match> code;
+    int n = 0;
+    float numW[3], denW[3];
+    std::vector<float> g[3];
+};
+
+// Block matching and collaborative filtering of the reference blocks at (js[r], is[c]) for rows
+// r of a band, computed on `workers` threads, then scattered one block at a time in the scan
+// order of BM3D_Process_Base::Kernel (source/BM3D_Base.cpp:290-470), so the sums are the
+// reference's sequential ones whatever the number of workers.  match(j, i) gives the list,
+// planes(c, src, ref, stride) the planes of component c and acc_of(c) its accumulators.
+template <class Match_, class Planes, class AccOf>
+static void filter_blocks(const Job &job, const std::vector<int> &js, const std::vector<int> &is,
+                          int workers, Match_ &&match, Planes &&planes, AccOf &&acc_of, Stats *st)
+{
+    const Para &p = job.p;
+    std::vector<std::vector<float>> scratch(std::max(1, workers));
+    auto compute = [&](BlockOut &o, int j, int i, int w) {
+        o.code = match(j, i);
+        for (int c = 0; c < 3; ++c) {
+            if (!job.process[c]) continue;
+            const float *const *s1;
+            const float *const *r1;
+            ptrdiff_t stride;
+            planes(c, s1, r1, stride);
+            if (!p.wiener) o.n = cf_basic_filter(job.pd[c], p.G, p.B, o.code, s1, stride, o.g[c], o.numW[c], o.denW[c], st);
+            else o.n = cf_final_filter(job.pd[c], p.G, p.B, o.code, s1, r1, stride, o.g[c], scratch[w], job.wiener_mode, o.numW[c], o.denW[c], st);
+        }
+    };
+    auto put = [&](const BlockOut &o) {
+        for (int c = 0; c < 3; ++c)
+            if (job.process[c]) scatter(o.g[c].data(), o.code, o.n, p.B, acc_of(c), o.numW[c], o.denW[c]);
+    };
+    if (workers <= 1) {
+        BlockOut o;
+        for (int j : js)
+            for (int i : is) {
+                compute(o, j, i, 0);
+                put(o);
+            }
+        return;
+    }
+    const size_t band_rows = 4;
+    std::vector<BlockOut> out;
+    for (size_t r0 = 0; r0 < js.size(); r0 += band_rows) {
+        const size_t r1 = std::min(js.size(), r0 + band_rows);
+        const int nb = (int)((r1 - r0) * is.size());
+        out.resize(nb);
+        parallel_for(nb, workers, [&](int b, int w) { compute(out[b], js[r0 + b / is.size()], is[b % is.size()], w); });
+        for (int b = 0; b < nb; ++b) put(out[b]);
+    }
 }
 
 // BM3D_Process_Base::Kernel (source/BM3D_Base.cpp:290-470) on float planes.  dst planes are
 // used as the numerator accumulators (ResNum aliases dst in the reference).
 static void bm3d_frame(const Job &job, int H, int W, ptrdiff_t stride, const float *const src[3],
-                       const float *const ref[3], float *const dst[3])
+                       const float *const ref[3], float *const dst[3], int workers = 1, Stats *st = nullptr)
 {
     const Para &p = job.p;
     std::vector<float> den[3];
@@ -800,19 +969,12 @@ static void bm3d_frame(const Job &job, int H, int W, ptrdiff_t stride, const flo
     std::vector<int> js, is;
     scan_positions(H, p.B, p.step, js);
     scan_positions(W, p.B, p.step, is);
-    std::vector<float> buf;
-    for (int j : js)
-        for (int i : is) {
-            std::vector<Match> code = bm3d_match(p, ref[0], H, W, stride, j, i);
-            for (int c = 0; c < 3; ++c) {
-                if (!job.process[c]) continue;
-                Accum acc{dst[c], den[c].data(), 0, stride};
-                const float *s1[1] = {src[c]};
-                const float *r1[1] = {ref[c]};
-                if (!p.wiener) cf_basic(job.pd[c], p.G, p.B, code, s1, stride, acc, buf);
-                else cf_final(job.pd[c], p.G, p.B, code, s1, r1, stride, acc, buf, job.wiener_mode);
-            }
-        }
+    const float *s1[3][1] = {{src[0]}, {src[1]}, {src[2]}};
+    const float *r1[3][1] = {{ref[0]}, {ref[1]}, {ref[2]}};
+    filter_blocks(job, js, is, workers,
+                  [&](int j, int i) { return bm3d_match(p, ref[0], H, W, stride, j, i, st); },
+                  [&](int c, const float *const *&s, const float *const *&r, ptrdiff_t &ld) { s = s1[c]; r = r1[c]; ld = stride; },
+                  [&](int c) { return Accum{dst[c], den[c].data(), 0, stride}; }, st);
     for (int c = 0; c < 3; ++c) {
         if (!job.process[c]) continue;
         for (int y = 0; y < H; ++y)
@@ -826,7 +988,7 @@ static void bm3d_frame(const Job &job, int H, int W, ptrdiff_t stride, const flo
 // VBM3D_Process_Base::BlockMatching (source/VBM3D_Base.cpp:540-659).  refs[f] is frame f of
 // the window, cur the index of the current frame in it.
 static std::vector<Match> vbm3d_match(const Para &p, const float *const *refs, int frames, int cur,
-                                      int H, int W, ptrdiff_t stride, int j, int i)
+                                      int H, int W, ptrdiff_t stride, int j, int i, Stats *st = nullptr)
 {
     if (p.G == 1 || p.thMSE <= 0) return std::vector<Match>(1, Match{0.0f, cur, j, i});
     std::vector<Match> code = bm_range(refs[cur], H, W, stride, j, i, p.B, p.R, p.bmstep,
@@ -853,9 +1015,25 @@ static std::vector<Match> vbm3d_match(const Para &p, const float *const *refs, i
             all.insert(all.end(), fm.begin(), fm.end());
         }
     }
+    bool ties = false;
     if (p.G > 0 && (int)all.size() > p.G) {
         std::partial_sort(all.begin() + 1, all.begin() + p.G, all.end());
+        if (st) {
+            float best = std::numeric_limits<float>::infinity();
+            for (size_t k = p.G; k < all.size(); ++k) best = std::min(best, all[k].key);
+            std::vector<float> kept;
+            for (int k = 0; k < p.G; ++k) kept.push_back(all[k].key);
+            ties = has_tie(kept, best, true, 1);
+        }
         all.resize(p.G);
+    } else if (st) {
+        std::vector<float> kept;
+        for (const Match &m : all) kept.push_back(m.key);
+        ties = has_tie(kept, 0.0f, false, 1);
+    }
+    if (st) {
+        st->blocks += 1;
+        st->tie_blocks += ties;
     }
     return all;
 }
@@ -865,7 +1043,7 @@ static std::vector<Match> vbm3d_match(const Para &p, const float *const *refs, i
 // frame f (source/VBM3D_Base.cpp:697-720).
 static void vbm3d_frame(const Job &job, int H, int W, ptrdiff_t stride, int frames, int cur,
                         int b_offset, const float *const *src[3], const float *const *ref[3],
-                        float *const dst[3])
+                        float *const dst[3], int workers = 1, Stats *st = nullptr)
 {
     const Para &p = job.p;
     const ptrdiff_t pc = (ptrdiff_t)H * stride;
@@ -875,18 +1053,13 @@ static void vbm3d_frame(const Job &job, int H, int W, ptrdiff_t stride, int fram
     std::vector<int> js, is;
     scan_positions(H, p.B, p.step, js);
     scan_positions(W, p.B, p.step, is);
-    std::vector<float> buf;
-    for (int j : js)
-        for (int i : is) {
-            std::vector<Match> code = vbm3d_match(p, ref[0], frames, cur, H, W, stride, j, i);
-            for (int c = 0; c < 3; ++c) {
-                if (!job.process[c]) continue;
-                float *base = dst[c] + pc * 2 * (p.radius + b_offset);
-                Accum acc{base, base + pc, 2 * pc, stride};
-                if (!p.wiener) cf_basic(job.pd[c], p.G, p.B, code, src[c], stride, acc, buf);
-                else cf_final(job.pd[c], p.G, p.B, code, src[c], ref[c], stride, acc, buf, job.wiener_mode);
-            }
-        }
+    filter_blocks(job, js, is, workers,
+                  [&](int j, int i) { return vbm3d_match(p, ref[0], frames, cur, H, W, stride, j, i, st); },
+                  [&](int c, const float *const *&s, const float *const *&r, ptrdiff_t &ld) { s = src[c]; r = ref[c]; ld = stride; },
+                  [&](int c) {
+                      float *base = dst[c] + pc * 2 * (p.radius + b_offset);
+                      return Accum{base, base + pc, 2 * pc, stride};
+                  }, st);
 }
 
 } // namespace orc
@@ -960,15 +1133,40 @@ void oracle_filter_tables(int wiener, double sigma_norm, int G, int B, double la
     }
 }
 
+// Statistics out: [0] groups filtered (per plane), [1] hard-threshold decisions, [2] decisions
+// that differ from an FP64 evaluation of the transform (Basic), [3] coefficients within a
+// relative 2^-10 of their threshold, [4] reference blocks matched, [5] blocks with tie events.
+static void put_stats(const Stats &st, long long *out)
+{
+    if (!out) return;
+    out[0] = st.groups; out[1] = st.coefs; out[2] = st.flips; out[3] = st.band;
+    out[4] = st.blocks; out[5] = st.tie_blocks;
+}
+
+// Splits `threads` into frame workers (one frame each, as VapourSynth's fmParallel runs frames)
+// and, when there are fewer frames than threads, workers inside each frame.
+static void split_threads(int threads, int nframes, int &frame_workers, int &intra)
+{
+    if (threads < 1) threads = 1;
+    frame_workers = std::max(1, std::min(threads, nframes));
+    intra = std::max(1, threads / frame_workers);
+}
+
 // BM3D over a batch of frames of float planes.  Layout [frame][plane][H][stride]; planes that
 // are not processed are copied through.  Frames run in parallel on `threads` host threads (one
-// frame per thread, as VapourSynth's fmParallel does); each frame is processed sequentially.
-int oracle_bm3d(const oracle_params *a, int nframes, int nplanes, int H, int W, int stride,
-                const float *src, const float *ref, float *dst, int threads)
+// frame per thread, as VapourSynth's fmParallel does); with fewer frames than threads, each frame
+// also splits its reference blocks over the spare threads (the aggregation stays sequential).
+// stats: null, or 6 counters (put_stats), which add an FP64 transform per group.
+int oracle_bm3d_ex(const oracle_params *a, int nframes, int nplanes, int H, int W, int stride,
+                   const float *src, const float *ref, float *dst, int threads, long long *stats)
 {
     Job job = make_job(a);
     if (nplanes == 1) { job.process[1] = job.process[2] = 0; }
     const size_t pc = (size_t)H * stride;
+    Stats st;
+    Stats *stp = stats ? &st : nullptr;
+    int fw, intra;
+    split_threads(threads, nframes, fw, intra);
     std::atomic<int> next(0);
     auto work = [&]() {
         for (;;) {
@@ -984,45 +1182,59 @@ int oracle_bm3d(const oracle_params *a, int nframes, int nplanes, int H, int W, 
             }
             for (int c = 0; c < nplanes; ++c)
                 if (!job.process[c]) std::memcpy(d[c], s[c], sizeof(float) * pc);
-            bm3d_frame(job, H, W, stride, s, r, d);
+            bm3d_frame(job, H, W, stride, s, r, d, intra, stp);
         }
     };
-    if (threads < 1) threads = 1;
     std::vector<std::thread> th;
-    for (int t = 1; t < threads; ++t) th.emplace_back(work);
+    for (int t = 1; t < fw; ++t) th.emplace_back(work);
     work();
     for (auto &t : th) t.join();
+    put_stats(st, stats);
     return 0;
 }
 
+int oracle_bm3d(const oracle_params *a, int nframes, int nplanes, int H, int W, int stride,
+                const float *src, const float *ref, float *dst, int threads)
+{
+    return oracle_bm3d_ex(a, nframes, nplanes, H, W, stride, src, ref, dst, threads, nullptr);
+}
+
 // Match lists of every reference block of one frame (debug/parity).  Row-major over the
-// ref-block scan; per block: count, then G entries (key, y, x).
-int oracle_bm3d_matches(const oracle_params *a, int H, int W, int stride, const float *refY,
-                        int *counts, int *ys, int *xs, float *keys)
+// ref-block scan; per block: count, then G entries (key, y, x).  Blocks are matched on `threads`
+// host threads; stats (null or 6 counters) receives [4] blocks and [5] blocks with tie events.
+int oracle_bm3d_matches_ex(const oracle_params *a, int H, int W, int stride, const float *refY,
+                           int *counts, int *ys, int *xs, float *keys, int threads, long long *stats)
 {
     Job job = make_job(a);
     std::vector<int> js, is;
     scan_positions(H, job.p.B, job.p.step, js);
     scan_positions(W, job.p.B, job.p.step, is);
-    size_t b = 0;
-    for (int j : js)
-        for (int i : is) {
-            std::vector<Match> code = bm3d_match(job.p, refY, H, W, stride, j, i);
-            counts[b] = (int)code.size();
-            for (size_t k = 0; k < code.size(); ++k) {
-                ys[b * job.p.G + k] = code[k].y;
-                xs[b * job.p.G + k] = code[k].x;
-                keys[b * job.p.G + k] = code[k].key;
-            }
-            ++b;
+    Stats st;
+    const int nb = (int)(js.size() * is.size());
+    parallel_for(nb, std::max(1, threads), [&](int b, int) {
+        const int j = js[b / is.size()], i = is[b % is.size()];
+        std::vector<Match> code = bm3d_match(job.p, refY, H, W, stride, j, i, stats ? &st : nullptr);
+        counts[b] = (int)code.size();
+        for (size_t k = 0; k < code.size(); ++k) {
+            ys[(size_t)b * job.p.G + k] = code[k].y;
+            xs[(size_t)b * job.p.G + k] = code[k].x;
+            keys[(size_t)b * job.p.G + k] = code[k].key;
         }
-    return (int)b;
+    });
+    put_stats(st, stats);
+    return nb;
+}
+
+int oracle_bm3d_matches(const oracle_params *a, int H, int W, int stride, const float *refY,
+                        int *counts, int *ys, int *xs, float *keys)
+{
+    return oracle_bm3d_matches_ex(a, H, W, stride, refY, counts, ys, xs, keys, 1, nullptr);
 }
 
 // V-BM3D match lists for one output frame n (debug/parity); entries carry the window frame z.
-int oracle_vbm3d_matches(const oracle_params *a, int nframes_total, int n, int H, int W, int stride,
-                         const float *refY_clip /*[F][H][stride]*/, int *counts, int *zs, int *ys,
-                         int *xs, float *keys)
+int oracle_vbm3d_matches_ex(const oracle_params *a, int nframes_total, int n, int H, int W, int stride,
+                            const float *refY_clip /*[F][H][stride]*/, int *counts, int *zs, int *ys,
+                            int *xs, float *keys, int threads, long long *stats)
 {
     Job job = make_job(a);
     const int r = job.p.radius;
@@ -1035,29 +1247,41 @@ int oracle_vbm3d_matches(const oracle_params *a, int nframes_total, int n, int H
     std::vector<int> js, is;
     scan_positions(H, job.p.B, job.p.step, js);
     scan_positions(W, job.p.B, job.p.step, is);
-    size_t b = 0;
-    for (int j : js)
-        for (int i : is) {
-            std::vector<Match> code = vbm3d_match(job.p, refs.data(), frames, cur, H, W, stride, j, i);
-            counts[b] = (int)code.size();
-            for (size_t k = 0; k < code.size(); ++k) {
-                zs[b * job.p.G + k] = code[k].z;
-                ys[b * job.p.G + k] = code[k].y;
-                xs[b * job.p.G + k] = code[k].x;
-                keys[b * job.p.G + k] = code[k].key;
-            }
-            ++b;
+    Stats st;
+    const int nb = (int)(js.size() * is.size());
+    parallel_for(nb, std::max(1, threads), [&](int b, int) {
+        const int j = js[b / is.size()], i = is[b % is.size()];
+        std::vector<Match> code = vbm3d_match(job.p, refs.data(), frames, cur, H, W, stride, j, i, stats ? &st : nullptr);
+        counts[b] = (int)code.size();
+        for (size_t k = 0; k < code.size(); ++k) {
+            zs[(size_t)b * job.p.G + k] = code[k].z;
+            ys[(size_t)b * job.p.G + k] = code[k].y;
+            xs[(size_t)b * job.p.G + k] = code[k].x;
+            keys[(size_t)b * job.p.G + k] = code[k].key;
         }
-    return (int)b;
+    });
+    put_stats(st, stats);
+    return nb;
+}
+
+int oracle_vbm3d_matches(const oracle_params *a, int nframes_total, int n, int H, int W, int stride,
+                         const float *refY_clip, int *counts, int *zs, int *ys, int *xs, float *keys)
+{
+    return oracle_vbm3d_matches_ex(a, nframes_total, n, H, W, stride, refY_clip, counts, zs, ys, xs, keys, 1, nullptr);
 }
 
 // V-BM3D for output frames [n0, n0+count) of a clip of nframes_total float frames.
 // src/ref clip layout [F][plane][H][stride]; dst layout [count][plane][(2r+1)*2][H][stride].
-int oracle_vbm3d(const oracle_params *a, int nframes_total, int n0, int count, int nplanes,
-                 int H, int W, int stride, const float *src, const float *ref, float *dst,
-                 int threads)
+// threads and stats as in oracle_bm3d_ex.
+int oracle_vbm3d_ex(const oracle_params *a, int nframes_total, int n0, int count, int nplanes,
+                    int H, int W, int stride, const float *src, const float *ref, float *dst,
+                    int threads, long long *stats)
 {
     Job job = make_job(a);
+    Stats st;
+    Stats *stp = stats ? &st : nullptr;
+    int fw, intra;
+    split_threads(threads, count, fw, intra);
     if (nplanes == 1) { job.process[1] = job.process[2] = 0; }
     const size_t pc = (size_t)H * stride;
     const int r = job.p.radius;
@@ -1087,15 +1311,22 @@ int oracle_vbm3d(const oracle_params *a, int nframes_total, int n0, int count, i
                 int cc = c < nplanes ? c : 0;
                 d3[c] = dst + ((size_t)k * nplanes + cc) * slots * pc;
             }
-            vbm3d_frame(job, H, W, stride, frames, cur, b_off, s3, r3, d3);
+            vbm3d_frame(job, H, W, stride, frames, cur, b_off, s3, r3, d3, intra, stp);
         }
     };
-    if (threads < 1) threads = 1;
     std::vector<std::thread> th;
-    for (int t = 1; t < threads; ++t) th.emplace_back(work);
+    for (int t = 1; t < fw; ++t) th.emplace_back(work);
     work();
     for (auto &t : th) t.join();
+    put_stats(st, stats);
     return 0;
+}
+
+int oracle_vbm3d(const oracle_params *a, int nframes_total, int n0, int count, int nplanes,
+                 int H, int W, int stride, const float *src, const float *ref, float *dst,
+                 int threads)
+{
+    return oracle_vbm3d_ex(a, nframes_total, n0, count, nplanes, H, W, stride, src, ref, dst, threads, nullptr);
 }
 
 // VAggregate_Process::Kernel (source/VAggregate.cpp:93-160) for output frame n.
@@ -1234,6 +1465,129 @@ void oracle_opp2rgb_float(const float *Y, const float *U, const float *V, int H,
             R[q] = Ry * yy + Ru * u + Rv * v + offR;
             Gp[q] = Gy * yy + Gv * v + offG;
             Bp[q] = By * yy + Bu * u + Bv * v + offB;
+        }
+}
+
+
+// Samples of 1 (uint8), 2 (uint16) or 4 (float) bytes.
+static float load_sample(const void *p, int bytes, size_t q)
+{
+    if (bytes == 1) return (float)((const uint8_t *)p)[q];
+    if (bytes == 2) return (float)((const uint16_t *)p)[q];
+    return ((const float *)p)[q];
+}
+
+static void store_sample(void *p, int bytes, size_t q, float v)
+{
+    if (bytes == 1) ((uint8_t *)p)[q] = (uint8_t)v;          // static_cast truncation
+    else if (bytes == 2) ((uint16_t *)p)[q] = (uint16_t)v;
+    else ((float *)p)[q] = v;
+}
+
+// Full-range quantisation of a format (GetQuanPara, include/Helper.h:286-351): integer formats
+// [0, 2^b - 1] with chroma neutral 2^(b-1); float luma [0, 1], chroma [-0.5, 0.5] around 0.
+struct Quan {
+    float floorY, ceilY, floorC, neutralC, ceilC;
+    bool pc_chroma;       // _IsPCChroma (include/Helper.h:363-372)
+};
+
+static Quan quan_full(int bytes, int bits)
+{
+    Quan q;
+    if (bytes == 4) {
+        q.floorY = 0.0f; q.ceilY = 1.0f; q.floorC = -0.5f; q.neutralC = 0.0f; q.ceilC = 0.5f;
+        q.pc_chroma = false;
+    } else {
+        int fl, ne, ce;
+        quan_int(bits, 1, 0, fl, ne, ce);
+        q.floorY = (float)fl; q.ceilY = (float)ce;
+        quan_int(bits, 1, 1, fl, ne, ce);
+        q.floorC = (float)fl; q.neutralC = (float)ne; q.ceilC = (float)ce;
+        q.pc_chroma = fl < ne && (fl + ce) % 2 == 1;
+    }
+    return q;
+}
+
+// MatrixConvert_RGB2YUV, OPP branch (include/Conversion.hpp:205-236), for any sample types
+// (RGB2OPP_Process::process_core, include/RGB2OPP.h:185-205; RGB2FloatYUV, Conversion.hpp:470-487):
+// full range on both sides; integer destinations get the +0.5 (+0.499999 for PC-range chroma)
+// rounding offset, and with clip the results are clipped to the destination range.
+void oracle_rgb2opp_any(const void *R, const void *G, const void *B, int in_bytes, int in_bits,
+                        void *Y, void *U, void *V, int out_bytes, int out_bits, int H, int W,
+                        int stride, int clip)
+{
+    const Quan s = quan_full(in_bytes, in_bits), d = quan_full(out_bytes, out_bits);
+    const bool dst_float = out_bytes == 4;
+    const float sRange = s.ceilY - s.floorY;
+    const float dRangeY = d.ceilY - d.floorY, dRangeC = d.ceilC - d.floorC;
+    const float gainY = dRangeY / (sRange * 3.0f);
+    float offsetY = -s.floorY * 3.0f * gainY + d.floorY;
+    if (!dst_float) offsetY += 0.5f;
+    const float gainU = dRangeC / (sRange * 2.0f);
+    const float gainV = dRangeC / (sRange * 4.0f);
+    float offsetC = d.neutralC;
+    if (!dst_float) offsetC += d.pc_chroma ? 0.499999f : 0.5f;
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const size_t q = (size_t)y * stride + x;
+            const float r = load_sample(R, in_bytes, q), g = load_sample(G, in_bytes, q), b = load_sample(B, in_bytes, q);
+            float t = (r + g + b) * gainY + offsetY;
+            store_sample(Y, out_bytes, q, clip ? clipf(t, d.floorY, d.ceilY) : t);
+            t = (r - b) * gainU + offsetC;
+            store_sample(U, out_bytes, q, clip ? clipf(t, d.floorC, d.ceilC) : t);
+            t = (r - g * 2.0f + b) * gainV + offsetC;
+            store_sample(V, out_bytes, q, clip ? clipf(t, d.floorC, d.ceilC) : t);
+        }
+}
+
+// ConvertToY, OPP branch (include/Conversion.hpp:103-116) into float, full range, no clip
+// (RGB2FloatY, Conversion.hpp:455-468): Basic's ref plane of an RGB clip.
+void oracle_rgb2y_any(const void *R, const void *G, const void *B, int in_bytes, int in_bits, int H, int W,
+                      int stride, float *Y)
+{
+    const Quan s = quan_full(in_bytes, in_bits);
+    const float sRange = s.ceilY - s.floorY;
+    const float gain = (1.0f - 0.0f) / (sRange * 3.0f);
+    const float offset = -s.floorY * 3.0f * gain + 0.0f;
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const size_t q = (size_t)y * stride + x;
+            Y[q] = (load_sample(R, in_bytes, q) + load_sample(G, in_bytes, q) + load_sample(B, in_bytes, q)) * gain + offset;
+        }
+}
+
+// MatrixConvert_YUV2RGB, OPP branch (include/Conversion.hpp:290-392, coefficients
+// include/Specification.h:253-269), for any sample types (OPP2RGB_Process::process_core,
+// include/OPP2RGB.h:185-205; FloatYUV2RGB, Conversion.hpp:489-506), full range.
+void oracle_opp2rgb_any(const void *Y, const void *U, const void *V, int in_bytes, int in_bits,
+                        void *R, void *G, void *B, int out_bytes, int out_bits, int H, int W,
+                        int stride, int clip)
+{
+    const Quan s = quan_full(in_bytes, in_bits), d = quan_full(out_bytes, out_bits);
+    const bool dst_float = out_bytes == 4;
+    const float dRange = d.ceilY - d.floorY;
+    const float gainY = dRange / (s.ceilY - s.floorY);
+    const float gainC = dRange / (s.ceilC - s.floorC);
+    float Ry = (float)1.0L, Ru = (float)1.0L, Rv = (float)(2.0L / 3.0L);
+    float Gy = (float)1.0L, Gu = (float)0.0L, Gv = (float)(-4.0L / 3.0L);
+    float By = (float)1.0L, Bu = (float)-1.0L, Bv = (float)(2.0L / 3.0L);
+    Ry *= gainY; Ru *= gainC; Rv *= gainC;
+    Gy *= gainY; Gu *= gainC; Gv *= gainC;
+    By *= gainY; Bu *= gainC; Bv *= gainC;
+    float oR = -s.floorY * Ry - s.neutralC * (Ru + Rv) + d.floorY;
+    float oG = -s.floorY * Gy - s.neutralC * (Gu + Gv) + d.floorY;
+    float oB = -s.floorY * By - s.neutralC * (Bu + Bv) + d.floorY;
+    if (!dst_float) { oR += 0.5f; oG += 0.5f; oB += 0.5f; }
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const size_t q = (size_t)y * stride + x;
+            const float yy = load_sample(Y, in_bytes, q), u = load_sample(U, in_bytes, q), v = load_sample(V, in_bytes, q);
+            float t = Ry * yy + Ru * u + Rv * v + oR;
+            store_sample(R, out_bytes, q, clip ? clipf(t, d.floorY, d.ceilY) : t);
+            t = Gy * yy + Gv * v + oG;
+            store_sample(G, out_bytes, q, clip ? clipf(t, d.floorY, d.ceilY) : t);
+            t = By * yy + Bu * u + Bv * v + oB;
+            store_sample(B, out_bytes, q, clip ? clipf(t, d.floorY, d.ceilY) : t);
         }
 }
 

@@ -17,6 +17,9 @@ REF_LIB = os.path.join(HERE, "_ref", "librefblock.so")
 _P = C.POINTER
 _F = _P(C.c_float)
 _I = _P(C.c_int)
+_L = _P(C.c_longlong)
+
+STAT_NAMES = ("groups", "coefficients", "flips_vs_fp64", "near_threshold", "blocks", "tie_blocks")
 
 
 class Params(C.Structure):
@@ -46,9 +49,15 @@ def lib():
         L.oracle_matrix_norms.argtypes = [C.c_int, _P(C.c_double)]
         L.oracle_filter_tables.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, _P(C.c_double), _F, _F]
         L.oracle_bm3d.argtypes = [_P(Params), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F, _F, _F, C.c_int]
+        L.oracle_bm3d_ex.argtypes = [_P(Params), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F, _F, _F, C.c_int, _L]
         L.oracle_bm3d_matches.argtypes = [_P(Params), C.c_int, C.c_int, C.c_int, _F, _I, _I, _I, _F]
+        L.oracle_bm3d_matches_ex.argtypes = [_P(Params), C.c_int, C.c_int, C.c_int, _F, _I, _I, _I, _F, C.c_int, _L]
         L.oracle_vbm3d_matches.argtypes = [_P(Params), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F, _I, _I, _I, _I, _F]
+        L.oracle_vbm3d_matches_ex.argtypes = [_P(Params), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F, _I, _I, _I, _I,
+                                              _F, C.c_int, _L]
         L.oracle_vbm3d.argtypes = [_P(Params), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F, _F, _F, C.c_int]
+        L.oracle_vbm3d_ex.argtypes = [_P(Params), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F, _F, _F,
+                                      C.c_int, _L]
         L.oracle_vaggregate.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _I, C.c_int, C.c_int, C.c_int, _F, _F]
         L.oracle_dct3d.argtypes = [_F, C.c_int, C.c_int, C.c_int]
         L.oracle_dct3d_scalar.argtypes = [_F, C.c_int, C.c_int, C.c_int]
@@ -57,6 +66,11 @@ def lib():
         L.oracle_float2int.argtypes = [_F, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.oracle_rgb2opp_float.argtypes = [_F, _F, _F, C.c_int, C.c_int, C.c_int, _F, _F, _F]
         L.oracle_opp2rgb_float.argtypes = [_F, _F, _F, C.c_int, C.c_int, C.c_int, _F, _F, _F]
+        V = C.c_void_p
+        L.oracle_rgb2opp_any.argtypes = [V, V, V, C.c_int, C.c_int, V, V, V, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, C.c_int]
+        L.oracle_opp2rgb_any.argtypes = L.oracle_rgb2opp_any.argtypes
+        L.oracle_rgb2y_any.argtypes = [V, V, V, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F]
         _lib = L
     return _lib
 
@@ -136,17 +150,32 @@ def scan(extent, B, step):
 
 # ---- processing ------------------------------------------------------------------------------
 
-def bm3d(p, src, ref=None, threads=1):
-    """src/ref: float32 [frames][planes][H][W].  Returns float32 output of the same shape."""
+def _stats_buf(stats):
+    return np.zeros(len(STAT_NAMES), np.int64) if stats else None
+
+
+def _stats_ptr(buf):
+    return buf.ctypes.data_as(_L) if buf is not None else None
+
+
+def _stats_dict(buf):
+    return {k: int(v) for k, v in zip(STAT_NAMES, buf)}
+
+
+def bm3d(p, src, ref=None, threads=1, stats=False):
+    """src/ref: float32 [frames][planes][H][W].  Returns float32 output of the same shape, and with
+    stats=True also the counters of STAT_NAMES (threshold decisions flipped against an FP64
+    evaluation of the transform, tie events of the block matching)."""
     src = np.ascontiguousarray(src, np.float32)
     ref = src if ref is None else np.ascontiguousarray(ref, np.float32)
     F, P, H, W = src.shape
     dst = np.zeros_like(src)
-    lib().oracle_bm3d(C.byref(p), F, P, H, W, W, fp(src), fp(ref), fp(dst), threads)
-    return dst
+    sb = _stats_buf(stats)
+    lib().oracle_bm3d_ex(C.byref(p), F, P, H, W, W, fp(src), fp(ref), fp(dst), threads, _stats_ptr(sb))
+    return (dst, _stats_dict(sb)) if stats else dst
 
 
-def bm3d_matches(p, refY):
+def bm3d_matches(p, refY, threads=1, stats=False):
     refY = np.ascontiguousarray(refY, np.float32)
     H, W = refY.shape
     nb = len(scan(H, p.B, p.step)) * len(scan(W, p.B, p.step))
@@ -154,11 +183,13 @@ def bm3d_matches(p, refY):
     ys = np.full(nb * p.G, -1, np.int32)
     xs = np.full(nb * p.G, -1, np.int32)
     ks = np.zeros(nb * p.G, np.float32)
-    lib().oracle_bm3d_matches(C.byref(p), H, W, W, fp(refY), ip(cnt), ip(ys), ip(xs), fp(ks))
-    return cnt, ys.reshape(nb, p.G), xs.reshape(nb, p.G), ks.reshape(nb, p.G)
+    sb = _stats_buf(stats)
+    lib().oracle_bm3d_matches_ex(C.byref(p), H, W, W, fp(refY), ip(cnt), ip(ys), ip(xs), fp(ks), threads, _stats_ptr(sb))
+    out = (cnt, ys.reshape(nb, p.G), xs.reshape(nb, p.G), ks.reshape(nb, p.G))
+    return (out, _stats_dict(sb)) if stats else out
 
 
-def vbm3d_matches(p, refY_clip, n):
+def vbm3d_matches(p, refY_clip, n, threads=1, stats=False):
     clip = np.ascontiguousarray(refY_clip, np.float32)
     F, H, W = clip.shape
     nb = len(scan(H, p.B, p.step)) * len(scan(W, p.B, p.step))
@@ -167,12 +198,15 @@ def vbm3d_matches(p, refY_clip, n):
     ys = np.full(nb * p.G, -1, np.int32)
     xs = np.full(nb * p.G, -1, np.int32)
     ks = np.zeros(nb * p.G, np.float32)
-    lib().oracle_vbm3d_matches(C.byref(p), F, n, H, W, W, fp(clip), ip(cnt), ip(zs), ip(ys), ip(xs), fp(ks))
+    sb = _stats_buf(stats)
+    lib().oracle_vbm3d_matches_ex(C.byref(p), F, n, H, W, W, fp(clip), ip(cnt), ip(zs), ip(ys), ip(xs), fp(ks),
+                                  threads, _stats_ptr(sb))
     g = p.G
-    return cnt, zs.reshape(nb, g), ys.reshape(nb, g), xs.reshape(nb, g), ks.reshape(nb, g)
+    out = (cnt, zs.reshape(nb, g), ys.reshape(nb, g), xs.reshape(nb, g), ks.reshape(nb, g))
+    return (out, _stats_dict(sb)) if stats else out
 
 
-def vbm3d(p, src, ref=None, n0=0, count=None, threads=1):
+def vbm3d(p, src, ref=None, n0=0, count=None, threads=1, stats=False):
     """src/ref: float32 [F][planes][H][W].  Returns [count][planes][(2r+1)*2*H][W] stacked output."""
     src = np.ascontiguousarray(src, np.float32)
     ref = src if ref is None else np.ascontiguousarray(ref, np.float32)
@@ -180,8 +214,9 @@ def vbm3d(p, src, ref=None, n0=0, count=None, threads=1):
     count = F - n0 if count is None else count
     slots = (2 * p.radius + 1) * 2
     dst = np.zeros((count, P, slots * H, W), np.float32)
-    lib().oracle_vbm3d(C.byref(p), F, n0, count, P, H, W, W, fp(src), fp(ref), fp(dst), threads)
-    return dst
+    sb = _stats_buf(stats)
+    lib().oracle_vbm3d_ex(C.byref(p), F, n0, count, P, H, W, W, fp(src), fp(ref), fp(dst), threads, _stats_ptr(sb))
+    return (dst, _stats_dict(sb)) if stats else dst
 
 
 def vaggregate(radius, stacked, process=(1, 1, 1)):
@@ -261,3 +296,42 @@ def ref_vbm3d_match(clip, cur, j, i, B, bm_range, bm_step, G, ps_num, ps_range, 
     n = ref().ref_vbm3d_match(arr, F, cur, H, W, W, j, i, B, bm_range, bm_step, G, ps_num, ps_range, ps_step,
                               thmse_norm, fp(k), ip(z), ip(y), ip(x), cap)
     return k[:n], z[:n], y[:n], x[:n]
+
+
+def _bits_of(a, bits):
+    return 32 if a.dtype == np.float32 else (bits or (8 if a.dtype == np.uint8 else 16))
+
+
+def rgb2opp_any(rgb, out_dtype=np.float32, in_bits=None, clip=None):
+    """MatrixConvert_RGB2YUV (OPP) for any sample types, full range: rgb [3][H][W] uint8/uint16/
+    float32 -> [3][H][W] of out_dtype.  clip defaults to "integer output" (RGB2OPP's rule)."""
+    rgb = np.ascontiguousarray(rgb)
+    H, W = rgb.shape[-2:]
+    out = np.zeros((3, H, W), out_dtype)
+    clip = (out.dtype != np.float32) if clip is None else clip
+    lib().oracle_rgb2opp_any(rgb[0].ctypes.data, rgb[1].ctypes.data, rgb[2].ctypes.data, rgb.itemsize,
+                             _bits_of(rgb, in_bits), out[0].ctypes.data, out[1].ctypes.data, out[2].ctypes.data,
+                             out.itemsize, _bits_of(out, None), H, W, W, int(clip))
+    return out
+
+
+def opp2rgb_any(yuv, out_dtype=np.float32, in_bits=None, clip=None):
+    """MatrixConvert_YUV2RGB (OPP) for any sample types, full range."""
+    yuv = np.ascontiguousarray(yuv)
+    H, W = yuv.shape[-2:]
+    out = np.zeros((3, H, W), out_dtype)
+    clip = (out.dtype != np.float32) if clip is None else clip
+    lib().oracle_opp2rgb_any(yuv[0].ctypes.data, yuv[1].ctypes.data, yuv[2].ctypes.data, yuv.itemsize,
+                             _bits_of(yuv, in_bits), out[0].ctypes.data, out[1].ctypes.data, out[2].ctypes.data,
+                             out.itemsize, _bits_of(out, None), H, W, W, int(clip))
+    return out
+
+
+def rgb2y_any(rgb, in_bits=None):
+    """ConvertToY (OPP) into float: the Y plane Basic matches on for an RGB ref clip."""
+    rgb = np.ascontiguousarray(rgb)
+    H, W = rgb.shape[-2:]
+    out = np.zeros((H, W), np.float32)
+    lib().oracle_rgb2y_any(rgb[0].ctypes.data, rgb[1].ctypes.data, rgb[2].ctypes.data, rgb.itemsize,
+                           _bits_of(rgb, in_bits), H, W, W, fp(out))
+    return out

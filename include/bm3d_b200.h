@@ -156,7 +156,8 @@ BM3D_API void bm3d_set_log_callback(bm3d_log_fn fn, void *user);
  * before any stream capture on the device.  All calls share the one array, which keeps the last
  * call's contents; each call clears what must start at zero, but calls that overlap on the GPU
  * (different streams, or host threads that do not order their calls) race and corrupt each
- * other's results, so order them on one stream. */
+ * other's results, so order them on one stream.  The set-up is not redone after a device reset:
+ * do not call cudaDeviceReset on a device after the first call on it. */
 BM3D_API int bm3d_basic_noalloc(const float *src, float *dst, int width, int height, int64_t stride,
                                 const char *profile, double sigma, void *cuda_stream);
 

@@ -84,6 +84,8 @@ ERRORS = [
     ("Basic", dict(input=clip(), hard_thr=0.0), "bm3d.Basic: Invalid \"hard_thr\" assigned, must be a positive floating point number"),
     ("Basic", dict(input=clip(), precision="fp16"), "bm3d.Basic: Invalid \"precision\" assigned, must be \"fp32\", \"tf32\" or \"learned\""),
     ("VFinal", dict(input=clip(), ref=clip(), precision="bf16"), "bm3d.VFinal: Invalid \"precision\" assigned, must be \"fp32\", \"tf32\" or \"learned\""),
+    ("VBasic", dict(input=clip(), aggregate=2), "bm3d.VBasic: Invalid \"aggregate\" assigned, must be 0 (stacked output) or 1 (aggregated output)"),
+    ("VFinal", dict(input=clip(), ref=clip(), aggregate=1, sample=2), "bm3d.VFinal: Invalid 'sample' assigned, must be 0 (integer sample type) or 1 (float sample type)"),
     ("Final", dict(input=clip(), ref=clip(), group_size=0), "bm3d.Final: Invalid \"group_size\" assigned, must be an integer in [1, 256]"),
     ("VBasic", dict(input=clip(), radius=17), "bm3d.VBasic: Invalid \"radius\" assigned, must be an integer in [1, 16]"),
     ("VBasic", dict(input=clip(), ps_num=9), "bm3d.VBasic: Invalid \"ps_num\" assigned, must be an integer in [1, group_size]"),
@@ -114,6 +116,9 @@ def test_argspec_errors():
     assert rc == capi.BM3D_ERR_ARG and "ref" in err
     rc, err = create("Basic", input=clip(), block_size=8.5)
     assert rc == capi.BM3D_ERR_ARG and "block_size" in err
+    # the aggregated-output extension belongs to VBasic / VFinal only
+    rc, err = create("Basic", input=clip(), aggregate=1)
+    assert rc == capi.BM3D_ERR_ARG and "aggregate" in err
 
 
 def test_first_error_wins_in_reference_order():

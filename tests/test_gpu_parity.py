@@ -257,3 +257,31 @@ def test_vfinal_16bit_pipeline(orc):
     o_final_f = orc.vaggregate(1, orc.vbm3d(pf, f, rf))
     o_final = np.stack([np.stack([orc.float2int(o_final_f[k, c], 16, True, c > 0) for c in range(3)]) for k in range(4)])
     assert np.abs(g_final.astype(np.int64) - o_final.astype(np.int64)).max() <= 1
+
+
+# ---- aggregated V-BM3D output (no stacked clip) -------------------------------------------------
+
+@pytest.mark.parametrize("sample", [1, 0])
+def test_vbasic_vfinal_aggregate_equals_chain(sample):
+    """VBasic / VFinal with aggregate=1 give VAggregate(radius, sample) of their stacked output,
+    for whole-clip batches and for single-frame requests (which filter the neighbouring reference
+    frames too)."""
+    nz, _ = synth.motion_frames(9, 5, 40, 56, 15.0, planes=3)
+    if sample == 1:
+        src = source(nz.astype(np.float32), "YUV")
+    else:
+        src = source(np.stack([np.stack([synth.to_u16(np.clip(nz[f, c], 0, 1)) for c in range(3)]) for f in range(5)]), "YUV")
+    chain_b = core.bm3d.VAggregate(core.bm3d.VBasic(src, radius=2, sigma=15.0), radius=2, sample=sample)
+    fused_b = core.bm3d.VBasic(src, radius=2, sigma=15.0, aggregate=1, sample=sample)
+    assert fused_b.height == 40 and fused_b.bits_per_sample == (32 if sample else 16)
+    cb = chain_b.numpy()
+    tol = TOL if sample == 1 else 1
+    for batch in (None, 1):
+        fb = core.bm3d.VBasic(src, radius=2, sigma=15.0, aggregate=1, sample=sample).numpy(batch)
+        assert np.abs(fb.astype(np.float64) - cb.astype(np.float64)).max() <= tol
+    f0 = fused_b.get_frame(0)
+    assert "BM3D_V_radius" not in f0.props and "BM3D_V_process" not in f0.props
+    ref = source(cb, "YUV")
+    chain_f = core.bm3d.VAggregate(core.bm3d.VFinal(src, ref, radius=2, sigma=15.0), radius=2, sample=sample).numpy()
+    fused_f = core.bm3d.VFinal(src, ref, radius=2, sigma=15.0, aggregate=1, sample=sample).numpy(2)
+    assert np.abs(fused_f.astype(np.float64) - chain_f.astype(np.float64)).max() <= tol

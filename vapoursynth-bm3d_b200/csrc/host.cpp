@@ -171,13 +171,15 @@ static const std::vector<ArgSpec> &argspec(const std::string &fn)
         {"block_step", 0, false, true}, {"group_size", 0, false, true}, {"bm_range", 0, false, true},
         {"bm_step", 0, false, true}, {"ps_num", 0, false, true}, {"ps_range", 0, false, true},
         {"ps_step", 0, false, true}, {"th_mse", 1, false, true}, {"hard_thr", 1, false, true},
-        {"matrix", 0, false, true}, {"precision", 2, false, true}};
+        {"matrix", 0, false, true}, {"precision", 2, false, true}, {"aggregate", 0, false, true},
+        {"sample", 0, false, true}};
     static const std::vector<ArgSpec> vfinal = {
         {"input", 3, false, false}, {"ref", 3, false, false}, {"profile", 2, false, true},
         {"sigma", 1, true, true}, {"radius", 0, false, true}, {"block_size", 0, false, true},
         {"block_step", 0, false, true}, {"group_size", 0, false, true}, {"bm_range", 0, false, true},
         {"bm_step", 0, false, true}, {"ps_num", 0, false, true}, {"ps_range", 0, false, true},
-        {"ps_step", 0, false, true}, {"th_mse", 1, false, true}, {"matrix", 0, false, true}, {"precision", 2, false, true}};
+        {"ps_step", 0, false, true}, {"th_mse", 1, false, true}, {"matrix", 0, false, true}, {"precision", 2, false, true},
+        {"aggregate", 0, false, true}, {"sample", 0, false, true}};
     static const std::vector<ArgSpec> vagg = {
         {"input", 3, false, false}, {"radius", 0, false, true}, {"sample", 0, false, true}};
     static const std::vector<ArgSpec> none;
@@ -729,6 +731,10 @@ public:
     bool vbm3d = false;
     bool tc = false;            // precision form: tensor-core transforms (argument "precision")
     bool learned = false;       // precision "learned": block matching by learned proposals
+    // extension of VBasic / VFinal: aggregate = 1 returns VAggregate(radius, sample) of the
+    // filter's output directly, without the stacked clip
+    bool aggregate = false;
+    int agg_sample = 0;
     DevBuf prop_wt;             // proposal network weights (device)
     PropBuffers prop_bufs;
     double plane_sigma[3] = {0, 0, 0};
@@ -865,6 +871,20 @@ public:
             if (pr == "tf32") tc = true;
             else if (pr == "learned") tc = learned = true;
             else if (pr != "fp32") return fail(BM3D_ERR_ARG, err("Invalid \"precision\" assigned, must be \"fp32\", \"tf32\" or \"learned\""));
+        }
+        if (vbm3d) {
+            const int64_t ag = map_get_int64(in, "aggregate", 0, &error);
+            if (!error) {
+                if (ag != 0 && ag != 1)
+                    return fail(BM3D_ERR_ARG, err("Invalid \"aggregate\" assigned, must be 0 (stacked output) or 1 (aggregated output)"));
+                aggregate = ag == 1;
+            }
+            const int64_t sm = map_get_int64(in, "sample", 0, &error);
+            if (!error) {
+                if (sm != 0 && sm != 1)
+                    return fail(BM3D_ERR_ARG, err("Invalid 'sample' assigned, must be 0 (integer sample type) or 1 (float sample type)"));
+                agg_sample = (int)sm;
+            }
         }
         return BM3D_OK;
     }
@@ -1358,18 +1378,36 @@ public:
             return fail(BM3D_ERR_UNSUPPORTED, err("radius beyond the supported maximum"));
         ovi = vi;
         ovi.color_family = vi.color_family == BM3D_RGB ? BM3D_YUV : vi.color_family;
-        ovi.sample_type = BM3D_FLOAT;
-        ovi.bits_per_sample = 32;
-        ovi.height = vi.height * (para.radius * 2 + 1) * 2;
+        if (aggregate) {
+            // the output of VAggregate(radius, sample) applied to the stacked clip
+            // (source/VAggregate.cpp, VAggregate_Create): same size, 16-bit or float
+            ovi.sample_type = agg_sample;
+            ovi.bits_per_sample = agg_sample == 1 ? 32 : 16;
+        } else {
+            ovi.sample_type = BM3D_FLOAT;
+            ovi.bits_per_sample = 32;
+            ovi.height = vi.height * (para.radius * 2 + 1) * 2;
+        }
         init_stream();
         return setup_device();
+    }
+
+    // Reference frames whose groups reach output frames [n, n + count): the frames themselves
+    // (stacked output), or every frame within the radius of one of them (aggregated output).
+    void ref_range(int n, int count, int *r0, int *cnt) const
+    {
+        const int r = aggregate ? para.radius : 0;
+        *r0 = std::max(0, n - r);
+        *cnt = std::min(vi.num_frames - 1, n + count - 1 + r) - *r0 + 1;
     }
 
     void window(int n, int count, int *first, int *num) const override
     {
         const int r = para.radius;
-        const int f0 = std::max(0, n - r);
-        const int f1 = std::min(vi.num_frames - 1, n + count - 1 + r);
+        int r0, rc;
+        ref_range(n, count, &r0, &rc);
+        const int f0 = std::max(0, r0 - r);
+        const int f1 = std::min(vi.num_frames - 1, r0 + rc - 1 + r);
         *first = f0;
         *num = f1 - f0 + 1;
     }
@@ -1388,15 +1426,21 @@ public:
             if (!frame_ok(dst[k], np)) return fail(BM3D_ERR_STATE, err("missing output frame planes"));
         const int r = para.radius;
         const int slots = 2 * r + 1;
-        ensure_ws(nwin, count);
-        const size_t nb = (size_t)sy.size() * sx.size() * count;
+        // reference frames [r0, r0 + rc) are filtered; their groups land in the accumulators of
+        // their window frames: per reference frame and window slot (stacked output), or per window
+        // frame of the batch (aggregated output: the sums over reference frames are VAggregate's)
+        int r0, rc;
+        ref_range(n, count, &r0, &rc);
+        const long long acc_planes = aggregate ? nwin : (long long)slots * rc;
+        ensure_ws(nwin, rc);
+        const size_t nb = (size_t)sy.size() * sx.size() * rc;
         v_pos.get(sizeof(uint32_t) * nb * para.G);
         v_n.get(sizeof(int) * nb);
         v_key.get(sizeof(float) * nb * para.G);
         for (int p = 0; p < 3; ++p)
             if (process[p] && p < np) {
-                acc_num[p].get(sizeof(float) * fs * slots * count);
-                acc_w[p].get(sizeof(float) * fs * slots * count);
+                acc_num[p].get(sizeof(float) * fs * acc_planes);
+                acc_w[p].get(sizeof(float) * fs * acc_planes);
             }
         CU(cudaMemsetAsync(stats, 0, 3 * sizeof(unsigned long long), stream));
         // window frames into the workspace; properties of each output frame's own source frame
@@ -1412,24 +1456,24 @@ public:
             if (rdef) ingest(*ref[i], true, i, fl);
         }
         mark(1);
-        // K1 on the current frames
-        run_bm(n - first, count, m_pos.as<uint32_t>(), m_n.as<int>(), m_key.as<float>());
+        // K1 on the reference frames
+        run_bm(r0 - first, rc, m_pos.as<uint32_t>(), m_n.as<int>(), m_key.as<float>());
         mark(2);
         // window tables
-        std::vector<int> winb(count), winl(count), winc(count), s0(count);
-        for (int k = 0; k < count; ++k) {
-            const int nn = n + k;
+        std::vector<int> winb(rc), winl(rc), winc(rc), s0(rc);
+        for (int k = 0; k < rc; ++k) {
+            const int nn = r0 + k;
             const int boff = -std::min(nn, r);
             const int foff = std::min(vi.num_frames - 1 - nn, r);
             winb[k] = nn + boff - first;
             winl[k] = foff - boff + 1;
             winc[k] = -boff;
-            s0[k] = r + boff;
+            s0[k] = aggregate ? winb[k] : r + boff;
         }
-        CU(cudaMemcpyAsync(d_winb.get(sizeof(int) * count), winb.data(), sizeof(int) * count, cudaMemcpyHostToDevice, stream));
-        CU(cudaMemcpyAsync(d_winl.get(sizeof(int) * count), winl.data(), sizeof(int) * count, cudaMemcpyHostToDevice, stream));
-        CU(cudaMemcpyAsync(d_winc.get(sizeof(int) * count), winc.data(), sizeof(int) * count, cudaMemcpyHostToDevice, stream));
-        CU(cudaMemcpyAsync(d_slot0.get(sizeof(int) * count), s0.data(), sizeof(int) * count, cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(d_winb.get(sizeof(int) * rc), winb.data(), sizeof(int) * rc, cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(d_winl.get(sizeof(int) * rc), winl.data(), sizeof(int) * rc, cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(d_winc.get(sizeof(int) * rc), winc.data(), sizeof(int) * rc, cudaMemcpyHostToDevice, stream));
+        CU(cudaMemcpyAsync(d_slot0.get(sizeof(int) * rc), s0.data(), sizeof(int) * rc, cudaMemcpyHostToDevice, stream));
         // K2
         VBMArgs va{};
         DevBuf *refws = rdef ? ws_ref : ws_src;
@@ -1470,18 +1514,53 @@ public:
         }
         if (warps < 1) return fail(BM3D_ERR_UNSUPPORTED, err("ps_num / ps_range too large for the predictive-search buffers"));
         va.warps = warps;
-        CU(launch_vbm_predict(va, count, smem, stream));
+        CU(launch_vbm_predict(va, rc, smem, stream));
         mark(3);
-        // K3+K4 into the window slots
+        // K3+K4 into the accumulators
         for (int p = 0; p < np; ++p)
             if (process[p]) {
-                CU(cudaMemsetAsync(acc_num[p].p, 0, sizeof(float) * fs * slots * count, stream));
-                CU(cudaMemsetAsync(acc_w[p].p, 0, sizeof(float) * fs * slots * count, stream));
+                CU(cudaMemsetAsync(acc_num[p].p, 0, sizeof(float) * fs * acc_planes, stream));
+                CU(cudaMemsetAsync(acc_w[p].p, 0, sizeof(float) * fs * acc_planes, stream));
             }
         const long long bpf = (long long)sy.size() * sx.size();
-        run_cf(bpf * count, bpf, v_pos.as<uint32_t>(), v_n.as<int>(), true, d_winb.as<int>(), d_slot0.as<int>(), slots, fs);
+        run_cf(bpf * rc, bpf, v_pos.as<uint32_t>(), v_n.as<int>(), true, d_winb.as<int>(), d_slot0.as<int>(),
+               aggregate ? 0 : slots, fs);
         mark(4);
-        // stacked output
+        if (aggregate) aggregated_output(n, count, first, src, dst);
+        else stacked_output(count, dst);
+        mark(5);
+        stager_.flush(stream);
+        mark(6);
+        for (int k = 0; k < count; ++k) {
+            const bm3d_frame *sf = src[n + k - first];
+            copy_props(sf, dst[k]);
+            if (vi.color_family == BM3D_RGB) dst[k]->prop_bm3d_opp = 1;
+            if (aggregate) {
+                // VAggregate deletes the V-BM3D properties (include/VAggregate.h:147-231)
+                dst[k]->prop_v_radius = -1;
+                dst[k]->prop_v_process_count = -1;
+            } else {
+                dst[k]->prop_v_radius = r;
+                dst[k]->prop_v_process_count = 3;
+                for (int p = 0; p < 3; ++p) dst[k]->prop_v_process[p] = process[p];
+            }
+        }
+        last_count = rc;
+        if (sync) {
+            CU(cudaStreamSynchronize(stream));
+            read_stats();
+            check_tc_status();
+            stager_.release();
+        }
+        return BM3D_OK;
+    }
+
+private:
+    // VBasic / VFinal stacked clip (VBM3D_Process_Base, include/VBM3D_Base.h:284-312): slot
+    // 2(r+k) numerator, 2(r+k)+1 denominator of window frame k
+    void stacked_output(int count, bm3d_frame *const *dst)
+    {
+        const int np = nplanes();
         const PlaneGeom go{W * 4, ovi.height};
         std::vector<PlanePtr> outs;
         for (int k = 0; k < count; ++k)
@@ -1505,31 +1584,58 @@ public:
         sa.H = H;
         sa.W = W;
         sa.B = para.B;
-        sa.slots = slots;
+        sa.slots = 2 * para.radius + 1;
         sa.out = upload_ptrs(ptr_out_, outs);
         CU(launch_vstack(sa, count, stream));
-        mark(5);
-        stager_.flush(stream);
-        mark(6);
-        for (int k = 0; k < count; ++k) {
-            const bm3d_frame *sf = src[n + k - first];
-            copy_props(sf, dst[k]);
-            if (vi.color_family == BM3D_RGB) dst[k]->prop_bm3d_opp = 1;
-            dst[k]->prop_v_radius = r;
-            dst[k]->prop_v_process_count = 3;
-            for (int p = 0; p < 3; ++p) dst[k]->prop_v_process[p] = process[p];
-        }
-        last_count = count;
-        if (sync) {
-            CU(cudaStreamSynchronize(stream));
-            read_stats();
-            check_tc_status();
-            stager_.release();
-        }
-        return BM3D_OK;
     }
 
-private:
+    // Aggregated output: frame m's accumulators already hold the sums over every reference frame
+    // within the radius (VAggregate_Process::Kernel, source/VAggregate.cpp:93-160); normalise them
+    // in place and convert to the output format (Float2Int to 16 bits, or float).  Planes that
+    // are not processed come out zero, as VAggregate writes them.
+    void aggregated_output(int n, int count, int first, const bm3d_frame *const *src, bm3d_frame *const *dst)
+    {
+        const int np = nplanes();
+        FinalizeArgs fa{};
+        float *agg[3] = {nullptr, nullptr, nullptr};
+        for (int p = 0; p < 3; ++p) {
+            fa.process[p] = process[p] && p < np;
+            if (!fa.process[p]) continue;
+            agg[p] = acc_num[p].as<float>() + (long long)(n - first) * fs;
+            fa.num[p] = agg[p];
+            fa.wmap[p] = acc_w[p].as<float>() + (long long)(n - first) * fs;
+            fa.out[p] = agg[p];
+        }
+        fa.frame_stride = fs;
+        fa.ld = ld;
+        fa.H = H;
+        fa.W = W;
+        fa.B = para.B;
+        CU(launch_finalize(fa, count, stream));
+        const PlaneGeom go{W * bytes_per_sample(ovi), H};
+        for (int k = 0; k < count; ++k) {
+            const bm3d_frame &sf = *src[n + k - first];
+            const int64_t opp = vi.color_family == BM3D_RGB ? 1 : (sf.prop_bm3d_opp < 0 ? 0 : sf.prop_bm3d_opp);
+            const bool full = (sf.prop_range < 0 || opp == 1) ? true : sf.prop_range != 0;
+            for (int p = 0; p < np; ++p) {
+                PlanePtr t = stager_.target(*dst[k], p, go);
+                if (!process[p]) {
+                    CU(cudaMemset2DAsync(t.ptr, t.stride, 0, (size_t)go.width_bytes, H, stream));
+                    continue;
+                }
+                std::vector<PlanePtr> a1{PlanePtr{agg[p] + (long long)k * fs, (long long)ld * 4}}, b1{t};
+                ConvProgram pr{};
+                if (agg_sample == 1) pr = raw_program(SK_F32, 1, W, H);
+                else {
+                    pr.mode = 0; pr.in_kind = SK_F32; pr.out_kind = SK_U16; pr.nin = pr.nout = 1; pr.W = W; pr.H = H;
+                    pr.op[0] = float2int_op(16, full, p > 0);
+                }
+                CU(launch_convert(pr, upload_ptrs(conv_in_[conv_i_], a1), upload_ptrs(conv_out_[conv_i_], b1), 1, stream));
+                conv_i_ = (conv_i_ + 1) % kConvSlots;
+            }
+        }
+    }
+
     bool frame_full_quiet(const bm3d_frame &fr) const
     {
         int64_t opp = fr.prop_bm3d_opp < 0 ? 0 : fr.prop_bm3d_opp;

@@ -24,6 +24,7 @@ namespace bm3d {
 // Every kernel launch of the library goes through a launcher below and is counted here.
 static std::atomic<unsigned long long> g_launches{0};
 unsigned long long launch_count() { return g_launches.load(); }
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 #define COUNT_LAUNCH() g_launches.fetch_add(1, std::memory_order_relaxed)
 
 cudaError_t upload_odd_tables(const float *host_odd_all)

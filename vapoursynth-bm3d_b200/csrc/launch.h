@@ -68,7 +68,9 @@ struct F64Args;
 size_t cf_fp64_smem(int B, int G);
 cudaError_t launch_cf_fp64(const CFArgs &a, const F64Args &f, cudaStream_t s);
 
-// Number of kernels launched by this library since load.
+// Number of kernels launched by this library since load; count_launch() adds one for a kernel
+// launched outside this translation unit.
 unsigned long long launch_count();
+void count_launch();
 
 }  // namespace bm3d

@@ -14,7 +14,9 @@
 // and every GPU that loads the library's device code holds it until the process exits.  All calls
 // share it and it keeps the contents of the last call, so each call clears the accumulators that
 // must start at zero, and two calls that overlap on the GPU (different streams, or threads that
-// do not order their calls) race with each other.
+// do not order their calls) race with each other.  The set-up of a device (the array's address
+// and the constant tables) is done once per process: a caller that resets the device
+// (cudaDeviceReset) after its first call gets a reloaded, zeroed array and must not call again.
 
 #include "bm3d_b200.h"
 
@@ -219,6 +221,7 @@ extern "C" BM3D_API int bm3d_basic_noalloc(const float *src, float *dst, int wid
         (e = cudaMemsetAsync(wm, 0, sizeof(float) * P, s)) != cudaSuccess)
         return set_error(BM3D_ERR_CUDA, cuda_text("accumulator clear", e));
     const int nscan = std::max(nby, nbx);
+    count_launch();
     noalloc_scan_kernel<<<(nscan + 255) / 256, 256, 0, s>>>(sy, nby, height - B, sx, nbx, width - B, para.step);
     if ((e = cudaGetLastError()) != cudaSuccess) return set_error(BM3D_ERR_CUDA, cuda_text("scan kernel launch", e));
 
@@ -252,6 +255,8 @@ extern "C" BM3D_API int bm3d_basic_noalloc(const float *src, float *dst, int wid
         smem = sizeof(float) * ((size_t)ba.win_h * ba.win_pitch + (size_t)warps * bm_warp_floats(ba.cand_cap, G, B, false));
         if (smem <= 200 * 1024) break;
     }
+    if (warps < 1)
+        return set_error(BM3D_ERR_UNSUPPORTED, "bm3d_basic_noalloc: bm_range / block_size too large for the shared-memory search window");
     if ((e = launch_bm_full(ba, 1, smem, s)) != cudaSuccess) return set_error(BM3D_ERR_CUDA, cuda_text("block matching", e));
 
     // collaborative filter with hard thresholding; per-plane tables of BM3D_FilterData

@@ -285,3 +285,26 @@ def test_vbasic_vfinal_aggregate_equals_chain(sample):
     chain_f = core.bm3d.VAggregate(core.bm3d.VFinal(src, ref, radius=2, sigma=15.0), radius=2, sample=sample).numpy()
     fused_f = core.bm3d.VFinal(src, ref, radius=2, sigma=15.0, aggregate=1, sample=sample).numpy(2)
     assert np.abs(fused_f.astype(np.float64) - chain_f.astype(np.float64)).max() <= tol
+
+
+# ---- the mvsfunc wrapper's call sequence ----------------------------------------------------------
+
+def test_mvsfunc_bm3d_call_pattern(orc):
+    """mvsfunc.BM3D(src, sigma=3.0, profile1="fast") on RGB float input (README.md:329-335), as the
+    wrapper issues it: RGB2OPP(sample=1) -> Basic(sigma=[3,3,3], profile='fast', matrix=100) ->
+    Final(opp, basic, same) -> OPP2RGB(sample=1)."""
+    nz, _ = synth.rgb_frames(17, 2, 72, 96, 3.0)
+    src = source(nz, "RGB")
+    opp = core.bm3d.RGB2OPP(src, 1)
+    basic = core.bm3d.Basic(opp, sigma=[3.0, 3.0, 3.0], profile="fast", matrix=100)
+    final = core.bm3d.Final(opp, basic, sigma=[3.0, 3.0, 3.0], profile="fast", matrix=100)
+    out = core.bm3d.OPP2RGB(final, 1)
+    g_basic, g_out = basic.numpy(), out.numpy()
+    o_opp = np.stack([orc.rgb2opp(nz[k]) for k in range(2)])
+    pb = orc.default_params(0, False, "fast", 3.0, matrix=100)
+    assert np.abs(g_basic - orc.bm3d(pb, o_opp)).max() <= TOL
+    pf = orc.default_params(1, False, "fast", 3.0, matrix=100)
+    o_final = orc.bm3d(pf, o_opp, g_basic)
+    o_out = np.stack([orc.opp2rgb(o_final[k]) for k in range(2)])
+    assert np.abs(g_out - o_out).max() <= 2 * TOL
+    assert out.color_family == bm3d_b200.RGB and out.bits_per_sample == 32

@@ -1,8 +1,11 @@
 """Build recipe for the in-tree shared library lib/libbm3d_b200.so (sm_100a).
 
 Compiles csrc/kernels.cu (every kernel), csrc/host.cpp (argument processing, filter objects,
-C ABI of include/bm3d_b200.h) and csrc/noalloc.cu (the allocation-free Basic entry point) with nvcc, linking the CUDA runtime statically so the library only
-needs the NVIDIA driver at run time.
+C ABI of include/bm3d_b200.h) and csrc/noalloc.cu (the allocation-free Basic entry point) with
+nvcc, linking the CUDA runtime statically so the library only needs the NVIDIA driver at run time.
+
+Where the VapourSynth SDK header (VapourSynth4.h) is installed, also builds the VapourSynth plugin
+lib/libbm3d_vs.so from vs/bm3d_vsplugin.cpp (linked against libbm3d_b200.so, found next to it).
 """
 import os
 import shutil
@@ -29,6 +32,40 @@ def nvcc_path():
     raise RuntimeError("nvcc not found")
 
 
+VS_SRC = os.path.join(HERE, "vs", "bm3d_vsplugin.cpp")
+VS_LIB = os.path.join(LIB_DIR, "libbm3d_vs.so")
+
+
+def vapoursynth_include():
+    """Directory holding VapourSynth4.h (pkg-config vapoursynth, then the usual prefixes), or None."""
+    try:
+        out = subprocess.run(["pkg-config", "--cflags-only-I", "vapoursynth"], capture_output=True, text=True)
+        dirs = [d[2:] for d in out.stdout.split() if d.startswith("-I")] if out.returncode == 0 else []
+    except OSError:
+        dirs = []
+    dirs += ["/usr/include/vapoursynth", "/usr/local/include/vapoursynth", "/usr/include", "/usr/local/include"]
+    for d in dirs:
+        if os.path.exists(os.path.join(d, "VapourSynth4.h")):
+            return d
+    return None
+
+
+def build_vs_plugin(verbose=False):
+    """Builds lib/libbm3d_vs.so when the VapourSynth SDK is present; returns its path or None."""
+    inc = vapoursynth_include()
+    if inc is None:
+        if verbose:
+            print("VapourSynth SDK (VapourSynth4.h) not found: plugin adapter not built", file=sys.stderr)
+        return None
+    cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-I" + inc,
+           "-I" + os.path.join(os.path.dirname(HERE), "include"), "-o", VS_LIB, VS_SRC,
+           "-L" + LIB_DIR, "-lbm3d_b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    return VS_LIB
+
+
 def needs_build():
     if not os.path.exists(LIB):
         return True
@@ -48,6 +85,7 @@ def build(force=False, verbose=False):
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True, cwd=CSRC)
     os.replace(LIB + ".tmp", LIB)
+    build_vs_plugin(verbose)
     return LIB
 
 

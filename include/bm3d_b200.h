@@ -222,6 +222,13 @@ BM3D_API int bm3d_proposal_train(const float *frames, int nframes, int width, in
 BM3D_API int bm3d_proposal_match(const float *frame, int width, int height, const float *weights, int block_step,
                                  int group_size, int bm_range, float th_sse, int nprop, int *counts, int *ys, int *xs,
                                  int capacity);
+/* Proposal sets of that matching (weights required): per reference block the nprop candidate
+ * indices (raster order of its search window; the trailing default (0, 0) candidate of the
+ * reference's search list is index (window size)) whose exact distances are taken, unused slots
+ * 0xffffffff; *overflow_blocks = blocks whose cut needed the exact bisection.  Returns the number
+ * of reference blocks. */
+BM3D_API int bm3d_debug_proposal_sets(const float *frame, int width, int height, const float *weights, int block_step,
+                                      int bm_range, int nprop, uint32_t *sets, int64_t *overflow_blocks, int capacity);
 
 #ifdef __cplusplus
 }

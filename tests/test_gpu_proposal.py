@@ -139,3 +139,58 @@ def test_learned_filter_psnr():
     print(f"PSNR exhaustive (tf32) {p_exh:.4f} dB, learned proposals {p_learn:.4f} dB")
     assert np.isfinite(p_learn)
     assert p_learn >= p_exh - 0.3
+
+
+def proposal_sets(x, w, step, R, nprop):
+    H, W = x.shape
+    cap = 1 << 14
+    sets = np.zeros(cap * nprop, np.uint32)
+    ovf = C.c_int64(0)
+    n = capi.lib().bm3d_debug_proposal_sets(fptr(x), W, H, fptr(w), step, R, nprop,
+                                            sets.ctypes.data_as(P(C.c_uint32)), C.byref(ovf), cap)
+    assert n > 0
+    return sets[:n * nprop].reshape(n, nprop), int(ovf.value)
+
+
+@pytest.mark.parametrize("kind", ["noisy", "flat"])
+def test_proposal_sets_are_the_best_nprop(kind):
+    """Every block's proposal set holds the nprop best candidates by descriptor distance (the
+    trailing default (0, 0) candidate included, the block itself excluded): no candidate outside
+    the set scores lower than one inside.  The flat frame makes most scores equal, so the cut of
+    the per-lane lists overflows and the exact bisection must run."""
+    H, W, R, step, nprop = 56, 72, 16, 4, 96
+    if kind == "noisy":
+        x = synth.gray_frames(21, 1, H, W, 20.0)[0][0, 0]
+    else:
+        x = np.full((H, W), 0.5, np.float32) + 1e-4 * np.random.default_rng(3).normal(size=(H, W)).astype(np.float32)
+    w = default_weights()
+    d = descriptors(x, w).astype(np.float64)
+    sets, ovf = proposal_sets(x, w, step, R, nprop)
+    if kind == "flat":
+        assert ovf > 0
+    ys, xs = synth_scan(H, step), synth_scan(W, step)
+    b = 0
+    for j in ys:
+        for i in xs:
+            t, bo = max(0, j - R), min(H - 8, j + R)
+            l, r = max(0, i - R), min(W - 8, i + R)
+            cy, cx = np.mgrid[t:bo + 1, l:r + 1]
+            cy = np.append(cy.ravel(), 0)
+            cx = np.append(cx.ravel(), 0)
+            sc = ((d[cy, cx] - d[j, i]) ** 2).sum(axis=1)
+            sc[:-1][(cy[:-1] == j) & (cx[:-1] == i)] = np.inf
+            got = sets[b][sets[b] != 0xFFFFFFFF].astype(np.int64)
+            assert len(got) == min(nprop, len(sc)) and len(set(got.tolist())) == len(got)
+            inside = np.zeros(len(sc), bool)
+            inside[got] = True
+            if (~inside).any():
+                assert sc[inside].max() <= sc[~inside].min() + 1e-5 * (1.0 + sc[~inside].min())
+            b += 1
+
+
+def synth_scan(extent, step, B=8):
+    out, j, last = [], 0, extent - B
+    while j < last + step:
+        out.append(min(j, last))
+        j += step
+    return out

@@ -90,7 +90,10 @@ struct BMArgs {
     uint32_t *out_pos;         // [frame][by][bx][G], packed (y << 16) | x
     int *out_n;                // [frame][by][bx]
     float *out_key;            // optional, [frame][by][bx][G]
-    unsigned long long *stats; // optional: [0] blocks that took the exact heap path
+    unsigned long long *stats; // optional: [0] blocks that took the exact heap path, [1] precision
+                               // forms: blocks that needed an exact fallback, [2] tensor-core time-outs
+    uint32_t *out_prop;        // optional (learned proposals): [frame][by][bx][nprop] candidate
+                               // indices of each block's proposal set, unused slots 0xffffffff
     int warps;                 // warps per CTA
     int win_h, win_pitch;      // shared window capacity
     int cand_cap;              // per-warp distance slots (>= lattice + 1)

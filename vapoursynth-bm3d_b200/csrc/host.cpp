@@ -2055,7 +2055,8 @@ BM3D_API int bm3d_debug_bm_tc_counts(bm3d_filter *h, int64_t *fallbacks, int64_t
 // range R, candidate step 1: the training targets and the recall reference.
 static void exhaustive_lists(const float *planes, long long fs, int ld, int W, int H, int nframes, int step, int G, int R,
                              float thsse, const int *dsy, const int *dsx, int nby, int nbx, uint32_t *pos, int *cnt,
-                             const void *desc, int nprop, cudaStream_t stream)
+                             const void *desc, int nprop, cudaStream_t stream, uint32_t *props = nullptr,
+                             unsigned long long *stats = nullptr)
 {
     BMArgs a{};
     a.ref = planes;
@@ -2076,7 +2077,8 @@ static void exhaustive_lists(const float *planes, long long fs, int ld, int W, i
     a.out_pos = pos;
     a.out_n = cnt;
     a.out_key = nullptr;
-    a.stats = nullptr;
+    a.stats = stats;
+    a.out_prop = props;
     a.cand_cap = (2 * R + 1) * (2 * R + 1) + 1;
     a.win_h = std::min(H, 2 * R + 8);
     size_t smem = 0;
@@ -2257,6 +2259,42 @@ BM3D_API int bm3d_proposal_match(const float *frame, int width, int height, cons
             ys[i] = (int)unpack_y(P[i]);
             xs[i] = (int)unpack_x(P[i]);
         }
+        return nb;
+    });
+}
+
+// Proposal sets of the learned matching of one GRAY plane (candidate step 1): for every reference
+// block (block step `step`, range R) the indices, in raster order of its search window, of the
+// nprop candidates it re-ranks exactly; unused slots 0xffffffff.  *overflow_blocks receives the
+// number of blocks whose cut needed the exact selection.
+BM3D_API int bm3d_debug_proposal_sets(const float *frame, int width, int height, const float *weights, int step, int R,
+                                      int nprop, uint32_t *sets, int64_t *overflow_blocks, int capacity)
+{
+    g_error.clear();
+    if (!frame || !weights || !sets || width < 8 || height < 8 || R < 1 || step < 1 || nprop < 1 || nprop > 128)
+        return fail(BM3D_ERR_STATE, "bad arguments");
+    return guarded([&]() -> int {
+        const std::vector<int> syh = scan_positions(height, 8, step), sxh = scan_positions(width, 8, step);
+        const int nby = (int)syh.size(), nbx = (int)sxh.size(), nb = nby * nbx;
+        if (nb > capacity) throw std::runtime_error("capacity too small");
+        const int G = 2;
+        DevBuf x, wt, dsy, dsx, lp, ln, pp, st;
+        PropBuffers pb;
+        CU(cudaMemcpy(x.get(sizeof(float) * width * height), frame, sizeof(float) * width * height, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(dsy.get(sizeof(int) * nby), syh.data(), sizeof(int) * nby, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(dsx.get(sizeof(int) * nbx), sxh.data(), sizeof(int) * nbx, cudaMemcpyHostToDevice));
+        CU(cudaMemcpy(wt.get(sizeof(float) * kProposalWeightCount), weights, sizeof(float) * kProposalWeightCount, cudaMemcpyHostToDevice));
+        CU(cudaMemset(st.get(4 * sizeof(unsigned long long)), 0, 4 * sizeof(unsigned long long)));
+        prop_descriptors(x.as<float>(), 0, width, width, height, 1, wt.as<float>(), pb, 0);
+        exhaustive_lists(x.as<float>(), 0, width, width, height, 1, step, G, R, 1e30f, dsy.as<int>(), dsx.as<int>(), nby, nbx,
+                         static_cast<uint32_t *>(lp.get(sizeof(uint32_t) * nb * G)), static_cast<int *>(ln.get(sizeof(int) * nb)),
+                         pb.desc.p, nprop, 0, static_cast<uint32_t *>(pp.get(sizeof(uint32_t) * (size_t)nb * nprop)),
+                         static_cast<unsigned long long *>(st.p));
+        CU(cudaDeviceSynchronize());
+        CU(cudaMemcpy(sets, pp.p, sizeof(uint32_t) * (size_t)nb * nprop, cudaMemcpyDeviceToHost));
+        unsigned long long h[4];
+        CU(cudaMemcpy(h, st.p, sizeof(h), cudaMemcpyDeviceToHost));
+        if (overflow_blocks) *overflow_blocks = (int64_t)h[1];
         return nb;
     });
 }

@@ -416,17 +416,40 @@ __global__ void __launch_bounds__(256) bm_learned_kernel(BMArgs a, const __nv_bf
     uint64_t cv[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) cv[e] = __shfl_sync(0xffffffffu, bb[e], pr & 31);
-    const uint64_t cut = cv[pr >> 5];
+    uint64_t cut = cv[pr >> 5];
     const unsigned lt = (1u << lane) - 1u;
-    int m = 0;
-    for (int c0 = 0; c0 < ctot; c0 += 32) {
-        const int c = c0 + lane;
-        const bool in = c < ctot && compose(sd[c], (uint32_t)c) <= cut;
-        const unsigned msk = __ballot_sync(0xffffffffu, in);
-        if (in && m + __popc(msk & lt) < 128) list[m + __popc(msk & lt)] = (uint32_t)c;
-        m += __popc(msk);
+    auto collect = [&]() {
+        int cnt = 0;
+        for (int c0 = 0; c0 < ctot; c0 += 32) {
+            const int c = c0 + lane;
+            const bool in = c < ctot && compose(sd[c], (uint32_t)c) <= cut;
+            const unsigned msk = __ballot_sync(0xffffffffu, in);
+            if (in && cnt + __popc(msk & lt) < 128) list[cnt + __popc(msk & lt)] = (uint32_t)c;
+            cnt += __popc(msk);
+        }
+        __syncwarp();
+        return cnt;
+    };
+    int m = collect();
+    if (m > 128) {
+        // More than 128 candidates at or below the cut (the union of per-lane lists can put it
+        // well above the true nprop-th score): the exact (pr + 1)-th smallest key by bisection over
+        // the composed (score, index) keys, which are distinct, so exactly pr + 1 lie at or below.
+        if (lane == 0 && a.stats) atomicAdd(a.stats + 1, 1ull);
+        uint64_t lo = 0, hi = cut;
+        while (lo < hi) {
+            const uint64_t mid = lo + ((hi - lo) >> 1);
+            int cnt = 0;
+            for (int c0 = 0; c0 < ctot; c0 += 32) {
+                const int c = c0 + lane;
+                cnt += __popc(__ballot_sync(0xffffffffu, c < ctot && compose(sd[c], (uint32_t)c) <= mid));
+            }
+            if (cnt >= pr + 1) hi = mid;
+            else lo = mid + 1;
+        }
+        cut = hi;
+        m = collect();
     }
-    __syncwarp();
     m = min(m, 128);
     if (m > pr + 1) {
         uint64_t sv[4];
@@ -441,6 +464,10 @@ __global__ void __launch_bounds__(256) bm_learned_kernel(BMArgs a, const __nv_bf
         for (int e = 0; e < 4; ++e) list[lane + 32 * e] = (uint32_t)sv[e];
         __syncwarp();
         m = pr + 1;
+    }
+    if (a.out_prop) {
+        uint32_t *op = a.out_prop + ob * nprop;
+        for (int e = lane; e < nprop; e += 32) op[e] = e < m ? list[e] : 0xffffffffu;
     }
     // exact distances of the proposals, valid ones ordered by (key, scan index)
     const float *rp = win + (j - wy0) * wp + (i - wx0);

@@ -193,6 +193,18 @@ BM3D_API int64_t bm3d_debug_slow_blocks(bm3d_filter *filter);
  * whose tensor-core wait timed out (their blocks also computed exactly).  No reference
  * counterpart.  Returns 0, or -1 for a null filter. */
 BM3D_API int bm3d_debug_bm_tc_counts(bm3d_filter *filter, int64_t *fallbacks, int64_t *timeouts);
+/* Precision form ("tf32"), hard threshold (Basic / VBasic), last call: coefficients whose
+ * tensor-core value lay within the recheck band of their threshold and were recomputed in fp32,
+ * and the keep / zero decisions that recomputation changed.  No reference counterpart (the
+ * reference's threshold rule is source/BM3D_Basic.cpp:98-134).  Returns 0, or -1. */
+BM3D_API int bm3d_debug_threshold_rechecks(bm3d_filter *filter, int64_t *rechecked, int64_t *changed);
+/* Sets that band (a fraction of each coefficient's threshold; 0 disables the recheck). */
+BM3D_API int bm3d_debug_set_recheck_band(bm3d_filter *filter, float band);
+/* Retained-coefficient count of every group of output frame k of the last call of a Basic
+ * filter (the count the reference turns into the group weight, source/BM3D_Basic.cpp:125-146),
+ * as counts[plane * nblocks + block] in reference-block scan order, -1 for planes not processed.
+ * Returns nblocks, or -1 (not a Basic filter, no such frame, capacity < 3 * nblocks). */
+BM3D_API int bm3d_debug_retained_counts(bm3d_filter *filter, int k, int *counts, int capacity);
 /* In-place 3-D transform of ngroups groups of n blocks of B x B floats in HOST memory (layout
  * [group][z][y][x]) using the device code of the collaborative filter; fast = 1 selects the
  * register path of the 8x8 / n in {8,16,32} kernels.  inverse = 0 forward (REDFT10 definition),

@@ -75,3 +75,40 @@ def test_precision_argument_is_validated():
     with pytest.raises(Exception) as e:
         core.bm3d.Basic(source(nz, "GRAY"), precision="fp16")
     assert "precision" in str(e.value)
+
+
+def flips(node_tc, node_plain, k):
+    """Sum over groups of |retained count (precision form) - retained count (plain path)|: a
+    lower bound of the keep / zero decisions that differ (exact unless one group flips both
+    ways)."""
+    a, b = node_tc.retained_counts(k), node_plain.retained_counts(k)
+    assert (a >= 0).sum() == (b >= 0).sum() > 0
+    m = b >= 0
+    return int(np.abs(a[m].astype(np.int64) - b[m]).sum()), int(b[m].sum())
+
+
+@pytest.mark.parametrize("sigma", [5.0, 10.0, 30.0])
+def test_hard_threshold_flips_counted(sigma):
+    """Hard-threshold decisions of the precision form against the plain path, on the same match
+    lists (the tensor-core matching is exact): without the near-threshold recheck the tf32
+    coefficients flip some decisions; with it every coefficient within the band is recomputed in
+    fp32 from the pixels and no decision differs."""
+    nz, _ = synth.gray_frames(55, 2, 540, 960, sigma)
+    clip = source(nz, "GRAY")
+    plain = core.bm3d.Basic(clip, profile="np", sigma=sigma)
+    plain.numpy()
+    raw = core.bm3d.Basic(clip, profile="np", sigma=sigma, precision="tf32")
+    raw.set_recheck_band(0.0)
+    raw.numpy()
+    tc = core.bm3d.Basic(clip, profile="np", sigma=sigma, precision="tf32")
+    tc.numpy()
+    f_raw = sum(flips(raw, plain, k)[0] for k in range(2))
+    f_tc, dec = 0, 0
+    for k in range(2):
+        f, d = flips(tc, plain, k)
+        f_tc += f
+    rechecked, changed = tc.threshold_rechecks()
+    kept = sum(int(plain.retained_counts(k)[0].sum()) for k in range(2))
+    print(f"sigma {sigma}: retained {kept}, flips without recheck {f_raw}, with recheck {f_tc}; "
+          f"recomputed {rechecked}, changed {changed}")
+    assert f_tc == 0

@@ -311,6 +311,27 @@ class FilterNode(VideoNode):
     def slow_blocks(self):
         return int(capi.lib().bm3d_debug_slow_blocks(self._h))
 
+    def threshold_rechecks(self):
+        """Precision form, hard threshold, last call: (coefficients recomputed in fp32 because their
+        tensor-core value lay near the threshold, keep / zero decisions that changed)."""
+        r, c = C.c_int64(0), C.c_int64(0)
+        capi.lib().bm3d_debug_threshold_rechecks(self._h, C.byref(r), C.byref(c))
+        return int(r.value), int(c.value)
+
+    def set_recheck_band(self, band):
+        if capi.lib().bm3d_debug_set_recheck_band(self._h, float(band)) != 0:
+            raise Error("not a BM3D / V-BM3D filter")
+
+    def retained_counts(self, k=0):
+        """Retained-coefficient count of every group of output frame k of the last computed batch
+        (Basic): int32 [3][blocks], -1 for planes not processed."""
+        cap = 3 * (1 << 21)
+        out = np.zeros(cap, np.int32)
+        nb = capi.lib().bm3d_debug_retained_counts(self._h, k, out.ctypes.data_as(C.POINTER(C.c_int)), cap)
+        if nb < 0:
+            raise Error("no retained counts for this filter / frame")
+        return out[:3 * nb].reshape(3, nb)
+
     def bm_tc_counts(self):
         """Precision-form block matching of the last call: (reference blocks that fell back to
         exact distances for every candidate, CTAs whose tensor-core wait timed out)."""

@@ -19,7 +19,8 @@ EXPORTS = [
     "bm3d_set_profiling", "bm3d_debug_stage_times", "bm3d_debug_launch_count", "bm3d_basic_noalloc",
     "bm3d_debug_reference_fp64", "bm3d_debug_bm_tc_counts", "bm3d_proposal_default_weights",
     "bm3d_proposal_descriptors", "bm3d_proposal_gradients", "bm3d_proposal_train", "bm3d_proposal_match",
-    "bm3d_debug_proposal_sets",
+    "bm3d_debug_proposal_sets", "bm3d_debug_threshold_rechecks", "bm3d_debug_set_recheck_band",
+    "bm3d_debug_retained_counts",
 ]
 
 
@@ -81,6 +82,9 @@ def lib():
                                       C.c_float, C.c_int, P(C.c_int), P(C.c_int), P(C.c_int), C.c_int]
     L.bm3d_debug_proposal_sets.argtypes = [P(C.c_float), C.c_int, C.c_int, P(C.c_float), C.c_int, C.c_int, C.c_int,
                                            P(C.c_uint32), P(C.c_int64), C.c_int]
+    L.bm3d_debug_threshold_rechecks.argtypes = [C.c_void_p, P(C.c_int64), P(C.c_int64)]
+    L.bm3d_debug_set_recheck_band.argtypes = [C.c_void_p, C.c_float]
+    L.bm3d_debug_retained_counts.argtypes = [C.c_void_p, C.c_int, P(C.c_int), C.c_int]
     L.bm3d_set_profiling.argtypes = [C.c_void_p, C.c_int]
     L.bm3d_debug_stage_times.argtypes = [C.c_void_p, P(C.c_double), C.c_int]
     L.bm3d_debug_launch_count.restype = C.c_int64

@@ -137,6 +137,14 @@ struct CFArgs {
     // device; the kernel then walks this list instead of every group
     const long long *plist;
     const unsigned int *plist_n;
+    // precision form, hard threshold: a coefficient whose tensor-core value lies within
+    // recheck_band * thr of its threshold is recomputed in fp32 from the pixels before the keep /
+    // zero decision (0 disables); tc_stats counts [0] coefficients recomputed, [1] decisions the
+    // recomputation changed
+    float recheck_band;
+    unsigned long long *tc_stats;
+    // optional (hard threshold): retained-coefficient count of every group, [plane][group]
+    int *retained;
 };
 
 struct VBMArgs {

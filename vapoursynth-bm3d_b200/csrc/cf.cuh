@@ -397,6 +397,8 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
                 if constexpr (!WIENER) kept += __shfl_xor_sync(0xffffffffu, kept, o);
                 else l2 = __fadd_rn(l2, __shfl_xor_sync(0xffffffffu, l2, o));
             }
+            if constexpr (!WIENER)
+                if (a.retained && inrange && !taken && z == 0) a.retained[(long long)p * a.ngroups + g0] = kept;
             __syncwarp();
 #pragma unroll
             for (int e = 0; e < 64; ++e) blk[e] = T[lane * kTP + e];

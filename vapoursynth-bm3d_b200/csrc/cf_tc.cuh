@@ -99,6 +99,15 @@ __host__ __device__ constexpr uint32_t tc_kmajor(int row, int k, int kdim)
 
 constexpr uint32_t kTcWaitLimit = 1u << 24;
 
+// mean of the 64 pixels of a block held two per lane by a warp
+__device__ __forceinline__ float block_mean(float v0, float v1)
+{
+    float s = v0 + v1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s * (1.0f / 64.0f);
+}
+
 template <int G, bool WIENER>
 __global__ void __launch_bounds__(TcShape<G, WIENER>::kTeam * TcShape<G, WIENER>::kWG, 1)
 cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
@@ -337,6 +346,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     };
     const int pfirst = next_plane(0);
     const long long tstride = (long long)gridDim.x * NWG;
+    // fp32 tables after the tensor-core image: C8[u][y] = 2 cos(pi (2y + 1) u / 16), then the
+    // z matrix Dz[kz][b] = 2 cos(pi (2b + 1) kz / 2G) (hard-threshold recheck and block means)
+    const float *xtab = reinterpret_cast<const float *>(reinterpret_cast<const unsigned char *>(tables) + Lay::kTableBytes);
+    unsigned long long n_recheck = 0, n_changed = 0;
 
     bool failed = false;
     Tile cur = fetch_tile((long long)blockIdx.x * NWG + wg);
@@ -356,6 +369,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             if (!a.process[p]) continue;
             const GroupLoc L = locate(a, p, g0, pk);
             const bool last = next_plane(p + 1) >= 3;
+            // hard threshold: every block enters the products with its mean removed, so that the
+            // tf32 rounding scales with the block's detail, not its level; the means' own
+            // transform (the (0, 0) coefficients) is added back exactly in fp32 before the threshold
+            float my_mu = 0.0f;
             // 1. gather (rows of foreign or partial groups are zero), one block per warp step
             if (region) {
                 if constexpr (Shp::kBoxes == 3) {
@@ -404,11 +421,19 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                                 v0 = Rg[(by + ry) * rp + bx + cx];
                                 v1 = Rg[(by + ry + 4) * rp + bx + cx];
                             }
+                            if constexpr (!WIENER) {
+                                const float mu = block_mean(v0, v1);
+                                v0 -= mu;
+                                v1 -= mu;
+                                if (lane == i) my_mu = mu;
+                                if constexpr (SPLIT == 2) if (lane == 0) part[b0 + i] = mu;
+                            }
                             *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane, 128)) = v0;
                             *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
                         }
                         tc::wg_sync(bar_id, TEAM);
                     }
+                    if constexpr (!WIENER && SPLIT == 2) my_mu = part[r];
                 }
             } else {
                 const float *sp = L.src + (long long)L.y * a.ld + L.x;
@@ -438,6 +463,22 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     }
                 }
                 tc::cp_async_wait_all();
+                if constexpr (!WIENER) {
+#pragma unroll 4
+                    for (int i = half * NI; i < half * NI + NI; ++i) {
+                        float *d0 = reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128));
+                        float *d1 = reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128));
+                        const float mu = block_mean(*d0, *d1);
+                        *d0 -= mu;
+                        *d1 -= mu;
+                        if (lane == i) my_mu = mu;
+                        if constexpr (SPLIT == 2) if (lane == 0) part[b0 + i] = mu;
+                    }
+                    if constexpr (SPLIT == 2) {
+                        tc::wg_sync(bar_id, TEAM);
+                        my_mu = part[r];
+                    }
+                }
             }
             if (last) {
                 bound_tile(nxt);
@@ -467,6 +508,16 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             float thr[3];                              // by the number of zero (y, x) frequencies
 #pragma unroll
             for (int k = 0; k < 3; ++k) thr[k] = WIENER ? 0.0f : a.thr4[p][G - 1][(j == 0) + k];
+            // (hard threshold) the exact z transform of the block means' (0, 0) coefficients 256 mu
+            float dcz = 0.0f;
+            uint64_t flags = 0;                        // columns (relative to cb) to recompute
+            if constexpr (!WIENER) {
+                const int gl = (lane / G) * G;         // lane of the group's first block
+#pragma unroll 4
+                for (int b = 0; b < G; ++b) dcz = fmaf(__ldg(xtab + 64 + j * G + b), __shfl_sync(0xffffffffu, my_mu, gl + b), dcz);
+                dcz *= 256.0f;
+            }
+            const float band = WIENER ? 0.0f : a.recheck_band;
 #pragma unroll
             for (int c0 = 0; c0 < NC; c0 += 32) {
                 float z[32];
@@ -487,16 +538,67 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     }
                 } else {
                     tc::tmem_wait_ld();
+                    if (cb + c0 == 0) z[0] += dcz;
 #pragma unroll
                     for (int e = 0; e < 32; ++e) {
                         const int c = cb + c0 + e;
-                        const bool keep = fabsf(z[e]) > thr[((c & 7) == 0) + ((c >> 3) == 0)];
+                        const float th = thr[((c & 7) == 0) + ((c >> 3) == 0)];
+                        const bool keep = fabsf(z[e]) > th;
+                        if (mine && fabsf(fabsf(z[e]) - th) <= band * th) flags |= 1ull << (c0 + e);
                         acc += keep ? 1.0f : 0.0f;
                         z[e] = keep ? z[e] : 0.0f;
                     }
                 }
 #pragma unroll
                 for (int e = 0; e < 32; ++e) *reinterpret_cast<float *>(D + tc::sw128_offset(cb + c0 + e, r, 64)) = z[e];
+            }
+            if constexpr (!WIENER) {
+                // coefficients near their threshold: the exact fp32 value from the pixels decides
+                // sum_b Dz[kz][b] sum_y C8[u][y] sum_x C8[v][x] x_b(y, x); the warp computes one
+                // at a time, lane = (pixel row y, every fourth block)
+                while (true) {
+                    const unsigned anyf = __ballot_sync(0xffffffffu, flags != 0ull);
+                    if (!anyf) break;
+                    const int ldr = __ffs(anyf) - 1;
+                    const uint64_t lf = __shfl_sync(0xffffffffu, flags, ldr);
+                    const int c = cb + __ffsll((long long)lf) - 1;
+                    const int u = c >> 3, v = c & 7, kz = ldr % G, gl = (ldr / G) * G;
+                    const int yy = lane & 7;
+                    float sum = 0.0f;
+#pragma unroll
+                    for (int k = 0; k < G / 4; ++k) {
+                        const int bb = (lane >> 3) + 4 * k;
+                        const float *px;
+                        long long pitch;
+                        if (region) {
+                            const int by = __shfl_sync(0xffffffffu, L.y, gl + bb) - y0, bx = __shfl_sync(0xffffffffu, L.x, gl + bb) - x0;
+                            px = Rg + (by + yy) * rp + bx;
+                            pitch = rp;
+                        } else {
+                            const float *sp = L.src + (long long)L.y * a.ld + L.x;
+                            px = reinterpret_cast<const float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(sp), gl + bb)) +
+                                 (long long)yy * a.ld;
+                            pitch = a.ld;
+                        }
+                        (void)pitch;
+                        float rs = 0.0f;
+#pragma unroll
+                        for (int x = 0; x < 8; ++x) rs = fmaf(__ldg(xtab + v * 8 + x), px[x], rs);
+                        sum = fmaf(__ldg(xtab + 64 + kz * G + bb) * __ldg(xtab + u * 8 + yy), rs, sum);
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+                    if (lane == ldr) {
+                        flags &= flags - 1;
+                        float *sv = reinterpret_cast<float *>(D + tc::sw128_offset(c, r, 64));
+                        const float th = thr[((c & 7) == 0) + ((c >> 3) == 0)];
+                        const bool keep_old = *sv != 0.0f, keep_new = fabsf(sum) > th;
+                        *sv = keep_new ? sum : 0.0f;
+                        acc += (keep_new ? 1.0f : 0.0f) - (keep_old ? 1.0f : 0.0f);
+                        ++n_recheck;
+                        n_changed += keep_new != keep_old;
+                    }
+                }
             }
 #pragma unroll
             for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -506,6 +608,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 tc::wg_sync(bar_id, TEAM);
                 acc = part[r] + part[r + 128];
             }
+            if constexpr (!WIENER)
+                if (a.retained && mine && j == 0 && half == 0) a.retained[(long long)p * a.ngroups + g0] = (int)acc;
             float denW;
             if constexpr (WIENER) {
                 const float eps = 1.1920928955078125e-07f;
@@ -626,6 +730,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     }
     tc::cp_async_wait_all();                          // no box copy outlives the kernel
     if (failed && t == 0) atomicExch(status, 1);
+    if (!WIENER && a.tc_stats && n_recheck) {
+        atomicAdd(a.tc_stats, n_recheck);
+        atomicAdd(a.tc_stats + 1, n_changed);
+    }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();

@@ -584,6 +584,7 @@ public:
                     bm3d_frame *const *dst, bool sync) = 0;
     virtual int matches(int, int *, int *, int *, int *, float *, int) { return -1; }
     virtual int reference_fp64(int, double *, long long) { return -1; }
+    virtual int retained(int, int *, int) { return -1; }
     // called after the filter's stream was synchronised (device-side error flags)
     virtual void synced() {}
     // the stats counters after the stream was synchronised
@@ -701,6 +702,12 @@ public:
 
 // ---------------------------------------------------------------------------------------------
 // Learned block-matching proposal: device buffers and the descriptor pass
+
+// Precision form, hard threshold: coefficients whose tensor-core value lies within this fraction
+// of their threshold are recomputed in fp32 before the keep / zero decision.  The tf32 products
+// of mean-free blocks stay well inside it (the test suite counts the decisions that still differ
+// from the plain path's at 1080p and 2160p).
+constexpr float kRecheckBand = 1.0f / 64.0f;
 
 // proposals per reference block that the learned form re-ranks exactly (of about 1,089 at range 16)
 constexpr int kLearnedProposals = 96;
@@ -918,6 +925,12 @@ public:
     DevBuf d_sy, d_sx, scratch;
     DevBuf d_winb, d_winl, d_winc, d_slot0;
     DevBuf tc_tab, tc_status, plist, plist_n;
+    // precision form, hard threshold: the recheck band (fraction of the threshold), the counters of
+    // the last call ([0] coefficients recomputed in fp32, [1] decisions changed) and the retained-
+    // coefficient count of every group of the last call ([plane][group])
+    float recheck_band = kRecheckBand;
+    DevBuf tc_counts, retained_buf;
+    unsigned long long last_tc_counts[2] = {0, 0};
     DirectTables dtabs;
     int last_count = 0;
 
@@ -938,6 +951,15 @@ public:
         if (tc && cf_tc_supported(para.B, para.G)) {
             std::vector<unsigned char> img;
             cf_tc_tables(para.G, img);
+            // fp32 tables of the hard-threshold recheck after the image: C8[u][y], Dz[kz][b]
+            std::vector<float> xt;
+            for (int u = 0; u < 8; ++u)
+                for (int y = 0; y < 8; ++y) xt.push_back(cos2((long)(2 * y + 1) * u, 16L));
+            for (int kz = 0; kz < para.G; ++kz)
+                for (int b = 0; b < para.G; ++b) xt.push_back(cos2((long)(2 * b + 1) * kz, 2L * para.G));
+            const size_t base = img.size();
+            img.resize(base + xt.size() * sizeof(float));
+            std::memcpy(img.data() + base, xt.data(), xt.size() * sizeof(float));
             CU(cudaMemcpy(tc_tab.get(img.size()), img.data(), img.size(), cudaMemcpyHostToDevice));
             CU(cudaMemset(tc_status.get(sizeof(int)), 0, sizeof(int)));
         }
@@ -953,6 +975,7 @@ public:
     // time-out flag of the tensor-core kernel (read after the stream is synchronised)
     void check_tc_status()
     {
+        if (tc_counts.p) CU(cudaMemcpy(last_tc_counts, tc_counts.p, sizeof(last_tc_counts), cudaMemcpyDeviceToHost));
         if (!tc_status.p) return;
         int st = 0;
         CU(cudaMemcpy(&st, tc_status.p, sizeof(int), cudaMemcpyDeviceToHost));
@@ -1130,7 +1153,15 @@ public:
         a.dtab = dtabs.tab.as<float>();
         a.dtab_off = dtabs.off.as<int>();
         const bool fast = cf_fast_supported(para.B, para.G);
+        if (!wiener) {
+            // retained counts of every group (inspection), written by the filter kernels
+            a.retained = static_cast<int *>(retained_buf.get(sizeof(int) * 3 * (size_t)std::max<long long>(1, ngroups)));
+            CU(cudaMemsetAsync(a.retained, 0xff, sizeof(int) * 3 * (size_t)std::max<long long>(1, ngroups), stream));
+        }
         if (fast && tc && tc_tab.p) {
+            a.recheck_band = recheck_band;
+            a.tc_stats = static_cast<unsigned long long *>(tc_counts.get(2 * sizeof(unsigned long long)));
+            CU(cudaMemsetAsync(a.tc_stats, 0, 2 * sizeof(unsigned long long), stream));
             // precision form: full groups on the tensor cores, partial ones on the plain kernel
             CU(launch_cf_tc(a, tc_tab.p, tc_status.as<int>(), stream));
             a.skip_full = 1;
@@ -1196,6 +1227,19 @@ public:
         for (int p = 0; p < 3; ++p)
             if (a.process[p]) CU(cudaMemcpy(out + p * plane_stride, f.num[p], sizeof(double) * pl, cudaMemcpyDeviceToHost));
         return 0;
+    }
+
+    // retained counts of frame k of the last call: [3][blocks per frame], -1 where not recorded
+    int retained(int k, int *out, int cap) override
+    {
+        if (vbm3d || wiener || k < 0 || k >= last_count || !retained_buf.p) return -1;
+        const size_t nb = sy.size() * sx.size();
+        if ((size_t)cap < 3 * nb) return -1;
+        CU(cudaStreamSynchronize(stream));
+        const size_t ng = nb * last_count;
+        for (int p = 0; p < 3; ++p)
+            CU(cudaMemcpy(out + p * nb, retained_buf.as<int>() + p * ng + k * nb, sizeof(int) * nb, cudaMemcpyDeviceToHost));
+        return (int)nb;
     }
 
     int matches(int k, int *counts, int *zs, int *ys, int *xs, float *keys, int cap) override
@@ -2047,6 +2091,31 @@ BM3D_API int bm3d_debug_bm_tc_counts(bm3d_filter *h, int64_t *fallbacks, int64_t
     if (fallbacks) *fallbacks = (int64_t)h->f->last_stats[1];
     if (timeouts) *timeouts = (int64_t)h->f->last_stats[2];
     return 0;
+}
+
+BM3D_API int bm3d_debug_threshold_rechecks(bm3d_filter *h, int64_t *rechecked, int64_t *changed)
+{
+    if (!h) return -1;
+    BM3DBase *b = dynamic_cast<BM3DBase *>(h->f.get());
+    if (!b) return -1;
+    if (rechecked) *rechecked = (int64_t)b->last_tc_counts[0];
+    if (changed) *changed = (int64_t)b->last_tc_counts[1];
+    return 0;
+}
+
+BM3D_API int bm3d_debug_set_recheck_band(bm3d_filter *h, float band)
+{
+    if (!h || !(band >= 0.0f)) return -1;
+    BM3DBase *b = dynamic_cast<BM3DBase *>(h->f.get());
+    if (!b) return -1;
+    b->recheck_band = band;
+    return 0;
+}
+
+BM3D_API int bm3d_debug_retained_counts(bm3d_filter *h, int k, int *counts, int capacity)
+{
+    if (!h || !counts) return -1;
+    return guarded([&]() -> int { return h->f->retained(k, counts, capacity); });
 }
 
 // ---- learned proposal: training and inspection -------------------------------------------------

@@ -112,3 +112,46 @@ def test_hard_threshold_flips_counted(sigma):
     print(f"sigma {sigma}: retained {kept}, flips without recheck {f_raw}, with recheck {f_tc}; "
           f"recomputed {rechecked}, changed {changed}")
     assert f_tc == 0
+
+
+def list_agreement(a, b, k, G):
+    ca, _, ya, xa, _ = a.matches(k, G)
+    cb, _, yb, xb, _ = b.matches(k, G)
+    m = np.arange(G)[None, :] < ca[:, None]
+    same = (ca == cb) & np.all(~m | ((ya == yb) & (xa == xb)), axis=1)
+    return float(same.mean())
+
+
+@pytest.mark.parametrize("sigma", [5.0, 15.0, 30.0])
+def test_precision_form_2160p(sigma):
+    """Gray float 3840x2160, 4 frames, profile 'np': the precision form against the plain path --
+    PSNR delta against the clean frames, match-list agreement, hard-threshold flips, and the error
+    of each stage's output against the FP64 recomputation of frame 0."""
+    nz, clean = synth.gray_frames(4, 4, 2160, 3840, sigma)
+    clip = source(nz, "GRAY")
+    res = {}
+    for prec in ("fp32", "tf32"):
+        b = core.bm3d.Basic(clip, profile="np", sigma=sigma, precision=prec)
+        f = core.bm3d.Final(clip, b, profile="np", sigma=sigma, precision=prec)
+        ob, of = b.numpy(), f.numpy()
+        eb = ob[0, 0].astype(np.float64) - b.reference_fp64(0)[0]
+        ef = of[0, 0].astype(np.float64) - f.reference_fp64(0)[0]
+        res[prec] = dict(b=b, f=f, ob=ob, of=of, eb=eb, ef=ef)
+    # the Final match lists with the plain Basic estimate as ref on both sides
+    ref = source(res["fp32"]["ob"], "GRAY")
+    fp = core.bm3d.Final(clip, ref, profile="np", sigma=sigma)
+    ft = core.bm3d.Final(clip, ref, profile="np", sigma=sigma, precision="tf32")
+    fp.compute(0, 1)
+    ft.compute(0, 1)
+    agree_b = list_agreement(res["tf32"]["b"], res["fp32"]["b"], 0, 16)
+    agree_f = list_agreement(ft, fp, 0, 32)
+    fl = sum(flips(res["tf32"]["b"], res["fp32"]["b"], k)[0] for k in range(4))
+    d_basic = psnr(res["tf32"]["ob"], clean) - psnr(res["fp32"]["ob"], clean)
+    d_final = psnr(res["tf32"]["of"], clean) - psnr(res["fp32"]["of"], clean)
+    stat = lambda e: f"rms {np.sqrt(np.mean(e * e)):.2e} max {np.abs(e).max():.2e}"
+    print(f"\n2160p sigma {sigma}: psnr plain {psnr(res['fp32']['of'], clean):.3f} dB, delta basic {d_basic:+.4f} "
+          f"final {d_final:+.4f} dB; list agreement basic {agree_b:.4f} final {agree_f:.4f}; flips {fl}; "
+          f"vs FP64 basic plain [{stat(res['fp32']['eb'])}] tf32 [{stat(res['tf32']['eb'])}], "
+          f"final plain [{stat(res['fp32']['ef'])}] tf32 [{stat(res['tf32']['ef'])}]")
+    assert agree_b == 1.0 and agree_f == 1.0
+    assert abs(d_final) <= PSNR_TOL_DB and fl == 0

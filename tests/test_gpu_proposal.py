@@ -194,3 +194,43 @@ def synth_scan(extent, step, B=8):
         out.append(min(j, last))
         j += step
     return out
+
+
+def list_recall(got, ref, G):
+    """Mean fraction of the exhaustive list's entries (z, y, x) that the other list also holds."""
+    cg, zg, yg, xg, _ = got
+    cr, zr, yr, xr, _ = ref
+    kg = (zg.astype(np.int64) << 32) | (yg.astype(np.int64) << 16) | xg
+    kr = (zr.astype(np.int64) << 32) | (yr.astype(np.int64) << 16) | xr
+    hits = 0.0
+    for b in range(len(cr)):
+        hits += len(set(kr[b, :cr[b]].tolist()) & set(kg[b, :cg[b]].tolist())) / cr[b]
+    return hits / len(cr)
+
+
+def test_learned_vbm3d_1080p_30_frames():
+    """V-BM3D with learned proposals in every frame of the window (the current frame's full search
+    and the other frames' predictive search): VBasic + VFinal, radius 2, 1920x1080 YUV444 float,
+    30 frames, sigma 20; group recall of the VBasic lists against the exhaustive search and PSNR of
+    the aggregated output against the exhaustive forms."""
+    F, H, W, sigma = 30, 1080, 1920, 20.0
+    nz, clean = synth.motion_frames(5, F, H, W, sigma, planes=3)
+    src = source(nz.astype(np.float32), "YUV")
+    clean = clean.astype(np.float64)
+    out, vb = {}, {}
+    for prec in ("fp32", "tf32", "learned"):
+        basic = core.bm3d.VBasic(src, radius=2, sigma=sigma, precision=prec, aggregate=1, sample=1)
+        final = core.bm3d.VFinal(src, basic, radius=2, sigma=sigma, precision=prec, aggregate=1, sample=1)
+        out[prec] = final.numpy(10)
+        v = core.bm3d.VBasic(src, radius=2, sigma=sigma, precision=prec)
+        v.compute(F // 2, 1)
+        vb[prec] = v.matches(0, 8)
+    ps = {k: 10 * np.log10(1.0 / np.mean((v.astype(np.float64) - clean) ** 2)) for k, v in out.items()}
+    rec = list_recall(vb["learned"], vb["fp32"], 8)
+    rec_tc = list_recall(vb["tf32"], vb["fp32"], 8)
+    print(f"\nlearned V-BM3D 1080p x{F}: PSNR fp32 {ps['fp32']:.3f}, tf32 {ps['tf32']:.3f}, learned {ps['learned']:.3f} dB "
+          f"(input {10 * np.log10(1.0 / np.mean((nz - clean) ** 2)):.3f}); VBasic group recall vs exhaustive: "
+          f"learned {rec:.4f}, tf32 {rec_tc:.4f}")
+    assert rec_tc == 1.0
+    assert rec >= 0.8
+    assert ps["learned"] - ps["fp32"] >= -0.1

@@ -171,6 +171,12 @@ struct VBMArgs {
     int warps;
     int sp_cap;                   // capacity of the per-warp search-position list
     int list_cap;                 // capacity of the per-warp concatenated list
+    // learned proposals (optional): bf16 descriptors of the window frames, desc_frame elements
+    // of kPropCh values per frame; the other frames' search positions are ranked by descriptor
+    // distance and only the best nprop get exact distances
+    const void *desc;
+    long long desc_frame;
+    int nprop;
 };
 
 struct PlanePtr {

@@ -711,6 +711,9 @@ constexpr float kRecheckBand = 1.0f / 64.0f;
 
 // proposals per reference block that the learned form re-ranks exactly (of about 1,089 at range 16)
 constexpr int kLearnedProposals = 96;
+// V-BM3D: proposals per reference block and other frame of the window, out of the predictive
+// search positions (up to ps_num * (2 ps_range + 1)^2, 162 to 242 with the default profiles)
+constexpr int kLearnedFrameProposals = 32;
 
 struct PropBuffers {
     DevBuf hid, feat, rs, desc, grad_d, dF, dH;
@@ -1051,8 +1054,18 @@ public:
         m_key.get(sizeof(float) * nb * para.G);
     }
 
-    // K1 over `nout` consecutive frames whose Y planes start at workspace slot `slot0`
-    void run_bm(int slot0, int nout, uint32_t *pos, int *cnt, float *key)
+    bool learned_matching() const { return learned && para.B == 8 && para.G >= 2 && para.G <= 32; }
+
+    void ensure_prop_weights()
+    {
+        if (!prop_wt.p)
+            CU(cudaMemcpy(prop_wt.get(sizeof(float) * kProposalWeightCount), kProposalWeights,
+                          sizeof(float) * kProposalWeightCount, cudaMemcpyHostToDevice));
+    }
+
+    // K1 over `nout` consecutive frames whose Y planes start at workspace slot `slot0`;
+    // desc_window: descriptors already computed for the workspace slots (learned form, V-BM3D)
+    void run_bm(int slot0, int nout, uint32_t *pos, int *cnt, float *key, const void *desc_window = nullptr)
     {
         DevBuf *refws = rdef ? ws_ref : ws_src;
         BMArgs a{};
@@ -1078,7 +1091,7 @@ public:
         const int lat = (2 * a.range / a.step + 1);
         a.cand_cap = lat * lat + 1;
         a.win_h = std::min(H, 2 * a.range + a.B);
-        const bool use_learned = learned && para.B == 8 && para.G >= 2 && para.G <= 32;
+        const bool use_learned = learned_matching();
         if (tc && !use_learned && para.B == 8 && a.step == 1 && para.G >= 2 && para.G <= 32) {
             // precision form: distance estimates on the tensor cores, exact lists
             const BmtLayout L = bmt_layout(a.range, H, para.step);
@@ -1101,13 +1114,16 @@ public:
         if (use_learned) {
             // learned proposals: descriptors of every block position, then the best
             // kLearnedProposals candidates by descriptor distance re-ranked with the exact SSD
-            if (!prop_wt.p) {
-                CU(cudaMemcpy(prop_wt.get(sizeof(float) * kProposalWeightCount), kProposalWeights,
-                              sizeof(float) * kProposalWeightCount, cudaMemcpyHostToDevice));
+            const void *desc = nullptr;
+            if (desc_window) {
+                desc = static_cast<const unsigned char *>(desc_window) + (size_t)slot0 * 2 * 16 * (size_t)(W - 7) * (H - 7);
+            } else {
+                ensure_prop_weights();
+                prop_descriptors(a.ref, fs, ld, W, H, nout, prop_wt.as<float>(), prop_bufs, stream);
+                desc = prop_bufs.desc.p;
             }
-            prop_descriptors(a.ref, fs, ld, W, H, nout, prop_wt.as<float>(), prop_bufs, stream);
             const size_t psmem = sizeof(float) * ((size_t)a.win_h * a.win_pitch + (size_t)a.warps * prop_warp_floats(a.cand_cap));
-            CU(launch_bm_learned(a, prop_bufs.desc.p, kLearnedProposals, nout, psmem, stream));
+            CU(launch_bm_learned(a, desc, kLearnedProposals, nout, psmem, stream));
             return;
         }
         CU(launch_bm_full(a, nout, smem, stream));
@@ -1500,8 +1516,16 @@ public:
             if (rdef) ingest(*ref[i], true, i, fl);
         }
         mark(1);
+        // learned form: descriptors of every window frame, for the current-frame proposals and
+        // for the other frames' predictive search
+        const void *dwin = nullptr;
+        if (learned_matching()) {
+            ensure_prop_weights();
+            prop_descriptors((rdef ? ws_ref : ws_src)[0].as<float>(), fs, ld, W, H, nwin, prop_wt.as<float>(), prop_bufs, stream);
+            dwin = prop_bufs.desc.p;
+        }
         // K1 on the reference frames
-        run_bm(r0 - first, rc, m_pos.as<uint32_t>(), m_n.as<int>(), m_key.as<float>());
+        run_bm(r0 - first, rc, m_pos.as<uint32_t>(), m_n.as<int>(), m_key.as<float>(), dwin);
         mark(2);
         // window tables
         std::vector<int> winb(rc), winl(rc), winc(rc), s0(rc);
@@ -1550,6 +1574,9 @@ public:
         const int wl = 2 * (va.ps_range / va.ps_step) + 1;
         va.sp_cap = para.psnum * wl * wl;
         va.list_cap = para.G * slots;
+        va.desc = dwin;
+        va.desc_frame = (long long)(W - 7) * (H - 7);
+        va.nprop = kLearnedFrameProposals;
         size_t smem = 0;
         int warps = 4;
         for (; warps >= 1; warps /= 2) {

@@ -18,6 +18,7 @@
 #include "select.cuh"
 #include "args.h"
 #include "bm.cuh"
+#include "proposal.cuh"
 
 namespace bm3d {
 
@@ -231,6 +232,12 @@ __global__ void __launch_bounds__(128) vbm_predict_kernel(VBMArgs a)
         for (int e = 0; e < 64; ++e) rb[e] = rblk[e];
     }
 
+    // learned proposals: descriptor of the reference block (current frame)
+    const __nv_bfloat16 *dsc = static_cast<const __nv_bfloat16 *>(a.desc);
+    const int Wd = a.W - 7;
+    float da[kPropCh];
+    if (dsc) load_desc(dsc + (long long)(wbase + cur) * a.desc_frame * kPropCh, (long long)j * Wd + i, da);
+
     // seeds from the current frame
     const int ncen0 = min(a.ps_num, n0);
     for (int k = lane; k < ncen0; k += 32) {
@@ -248,11 +255,51 @@ __global__ void __launch_bounds__(128) vbm_predict_kernel(VBMArgs a)
         for (int fz = cur + dir; fz >= 0 && fz < frames; fz += dir) {
             const int ns = gen_search_pos_warp(cen, ncen, a.H, a.W, B, a.ps_range, a.ps_step, sp, tmp, a.sp_cap);
             const float *plane = a.ref + (long long)(wbase + fz) * a.frame_stride;
-            for (int c = lane; c < ns; c += 32) {
-                const int y = unpack_y(sp[c]), x = unpack_x(sp[c]);
-                const float *src = plane + (long long)y * a.ld + x;
-                const float d = B == 8 ? ssd8_global(rb, src, a.ld) : ssd_any_global(rblk, B, src, a.ld);
-                sk[c] = dist_valid(d, a.thSSE) ? dist_to_key(d, a.distMul) : -1.0f;
+            if (dsc && B == 8 && ns > a.nprop) {
+                // learned proposals: the nprop positions of smallest descriptor distance (ties by
+                // position order) get exact distances, the others are left out of this frame's list
+                const __nv_bfloat16 *dz = dsc + (long long)(wbase + fz) * a.desc_frame * kPropCh;
+                uint64_t mx = 0;
+                for (int c = lane; c < ns; c += 32) {
+                    float dc[kPropCh];
+                    load_desc(dz, (long long)unpack_y(sp[c]) * Wd + unpack_x(sp[c]), dc);
+                    float sc = 0.0f;
+#pragma unroll
+                    for (int k = 0; k < kPropCh; ++k) sc = fmaf(da[k] - dc[k], da[k] - dc[k], sc);
+                    sk[c] = sc;
+                    mx = max(mx, compose(sc, (uint32_t)c));
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+                __syncwarp();
+                // the nprop-th smallest (score, index) key by bisection: the keys are distinct
+                uint64_t lo = 0, hi = mx;
+                while (lo < hi) {
+                    const uint64_t mid = lo + ((hi - lo) >> 1);
+                    int cnt = 0;
+                    for (int c0 = 0; c0 < ns; c0 += 32) {
+                        const int c = c0 + lane;
+                        cnt += __popc(__ballot_sync(0xffffffffu, c < ns && compose(sk[c], (uint32_t)c) <= mid));
+                    }
+                    if (cnt >= a.nprop) hi = mid;
+                    else lo = mid + 1;
+                }
+                __syncwarp();
+                for (int c = lane; c < ns; c += 32) {
+                    float key = -1.0f;
+                    if (compose(sk[c], (uint32_t)c) <= hi) {
+                        const float d = ssd8_global(rb, plane + (long long)unpack_y(sp[c]) * a.ld + unpack_x(sp[c]), a.ld);
+                        key = dist_valid(d, a.thSSE) ? dist_to_key(d, a.distMul) : -1.0f;
+                    }
+                    sk[c] = key;
+                }
+            } else {
+                for (int c = lane; c < ns; c += 32) {
+                    const int y = unpack_y(sp[c]), x = unpack_x(sp[c]);
+                    const float *src = plane + (long long)y * a.ld + x;
+                    const float d = B == 8 ? ssd8_global(rb, src, a.ld) : ssd_any_global(rblk, B, src, a.ld);
+                    sk[c] = dist_valid(d, a.thSSE) ? dist_to_key(d, a.distMul) : -1.0f;
+                }
             }
             __syncwarp();
             const int nf = select_positions(sk, ns, G, fk, fi);

@@ -99,22 +99,61 @@ __global__ void convert_kernel(ConvProgram pr, const PlanePtr *in, const PlanePt
 }
 
 
-__global__ void finalize_kernel(FinalizeArgs a)
+// Tile of the denominator (the B x B box sum of the per-origin weight map wm) for output rows
+// [ty0, ty0 + kFinTH) and columns [tx0, tx0 + kFinTW): the weight region with its (B - 1) halo is
+// staged in shared memory, summed along x, then along y (2B additions per pixel instead of B^2).
+// On return den[r * kFinTW + c] holds the denominator of pixel (ty0 + r, tx0 + c).
+constexpr int kFinTH = 32, kFinTW = 64;
+
+__host__ __device__ inline int finalize_smem_floats(int B)
 {
-    const int f = blockIdx.z;
-    const int p = blockIdx.y % 3;
+    return (kFinTH + B - 1) * (kFinTW + B - 1) + (kFinTH + B - 1) * kFinTW + kFinTH * kFinTW;
+}
+
+__device__ __forceinline__ float *box_den_tile(float *sm, const float *wm, int ld, int H, int W, int B, int ty0, int tx0)
+{
+    const int RH = kFinTH + B - 1, RW = kFinTW + B - 1;
+    float *reg = sm;
+    float *hs = sm + RH * RW;
+    float *den = hs + RH * kFinTW;
+    for (int e = threadIdx.x; e < RH * RW; e += blockDim.x) {
+        const int r = e / RW, c = e - r * RW;
+        const int yy = ty0 - (B - 1) + r, xx = tx0 - (B - 1) + c;
+        reg[e] = (yy >= 0 && xx >= 0 && yy < H && xx < W) ? wm[(long long)yy * ld + xx] : 0.0f;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < RH * kFinTW; e += blockDim.x) {
+        const int r = e / kFinTW, c = e - r * kFinTW;
+        float v = 0.0f;
+        for (int k = 0; k < B; ++k) v = __fadd_rn(v, reg[r * RW + c + k]);
+        hs[e] = v;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < kFinTH * kFinTW; e += blockDim.x) {
+        const int r = e / kFinTW, c = e - r * kFinTW;
+        float v = 0.0f;
+        for (int k = 0; k < B; ++k) v = __fadd_rn(v, hs[(r + k) * kFinTW + c]);
+        den[e] = v;
+    }
+    __syncthreads();
+    return den;
+}
+
+// grid (tiles along x, tiles along y, frames * 3 planes)
+__global__ void __launch_bounds__(256) finalize_kernel(FinalizeArgs a)
+{
+    extern __shared__ float fsm[];
+    const int f = blockIdx.z / 3, p = blockIdx.z % 3;
     if (!a.process[p]) return;
-    const int y = blockIdx.y / 3;
+    const int ty0 = blockIdx.y * kFinTH, tx0 = blockIdx.x * kFinTW;
     const long long fo = (long long)f * a.frame_stride;
-    const float *wm = a.wmap[p] + fo;
+    const float *den = box_den_tile(fsm, a.wmap[p] + fo, a.ld, a.H, a.W, a.B, ty0, tx0);
     const float *nm = a.num[p] + fo;
     float *o = a.out[p] + fo;
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < a.W; x += gridDim.x * blockDim.x) {
-        float den = 0.0f;
-        const int y0 = max(0, y - a.B + 1), x0 = max(0, x - a.B + 1);
-        for (int yy = y0; yy <= y; ++yy)
-            for (int xx = x0; xx <= x; ++xx) den = __fadd_rn(den, wm[(long long)yy * a.ld + xx]);
-        o[(long long)y * a.ld + x] = __fdiv_rn(nm[(long long)y * a.ld + x], den);
+    for (int e = threadIdx.x; e < kFinTH * kFinTW; e += blockDim.x) {
+        const int r = e / kFinTW, c = e - r * kFinTW;
+        const int y = ty0 + r, x = tx0 + c;
+        if (y < a.H && x < a.W) o[(long long)y * a.ld + x] = __fdiv_rn(nm[(long long)y * a.ld + x], den[e]);
     }
 }
 
@@ -141,26 +180,28 @@ __global__ void vaggregate_kernel(VAggArgs a)
     }
 }
 
-__global__ void vstack_kernel(VStackArgs a)
+// grid (tiles along x, slots * tiles along y, frames * 3 planes)
+__global__ void __launch_bounds__(256) vstack_kernel(VStackArgs a)
 {
+    extern __shared__ float fsm[];
     const int f = blockIdx.z / 3;
     const int p = blockIdx.z % 3;
     if (!a.process[p]) return;
-    const int s = blockIdx.y / a.H;
-    const int y = blockIdx.y - s * a.H;
+    const int tiles_y = (a.H + kFinTH - 1) / kFinTH;
+    const int s = blockIdx.y / tiles_y;
+    const int ty0 = (blockIdx.y - s * tiles_y) * kFinTH, tx0 = blockIdx.x * kFinTW;
     const long long so = ((long long)f * a.slots + s) * a.slot_stride;
-    const float *wm = a.wmap[p] + so;
+    const float *den = box_den_tile(fsm, a.wmap[p] + so, a.ld, a.H, a.W, a.B, ty0, tx0);
     const float *nm = a.num[p] + so;
     const PlanePtr &o = a.out[f * 3 + p];
-    float *nrow = reinterpret_cast<float *>(static_cast<char *>(o.ptr) + ((long long)(2 * s) * a.H + y) * o.stride);
-    float *drow = reinterpret_cast<float *>(static_cast<char *>(o.ptr) + ((long long)(2 * s + 1) * a.H + y) * o.stride);
-    for (int x = blockIdx.x * blockDim.x + threadIdx.x; x < a.W; x += gridDim.x * blockDim.x) {
-        float den = 0.0f;
-        const int y0 = max(0, y - a.B + 1), x0 = max(0, x - a.B + 1);
-        for (int yy = y0; yy <= y; ++yy)
-            for (int xx = x0; xx <= x; ++xx) den = __fadd_rn(den, wm[(long long)yy * a.ld + xx]);
+    for (int e = threadIdx.x; e < kFinTH * kFinTW; e += blockDim.x) {
+        const int r = e / kFinTW, c = e - r * kFinTW;
+        const int y = ty0 + r, x = tx0 + c;
+        if (y >= a.H || x >= a.W) continue;
+        float *nrow = reinterpret_cast<float *>(static_cast<char *>(o.ptr) + ((long long)(2 * s) * a.H + y) * o.stride);
+        float *drow = reinterpret_cast<float *>(static_cast<char *>(o.ptr) + ((long long)(2 * s + 1) * a.H + y) * o.stride);
         nrow[x] = nm[(long long)y * a.ld + x];
-        drow[x] = den;
+        drow[x] = den[e];
     }
 }
 

@@ -319,10 +319,12 @@ cudaError_t launch_convert(const ConvProgram &pr, const PlanePtr *in, const Plan
 
 cudaError_t launch_finalize(const FinalizeArgs &a, int nframes, cudaStream_t s)
 {
-    dim3 block(256);
-    dim3 grid((a.W + 255) / 256, a.H * 3, nframes);
+    const size_t smem = sizeof(float) * (size_t)finalize_smem_floats(a.B);
+    cudaError_t e;
+    if ((e = allow_smem(finalize_kernel, smem)) != cudaSuccess) return e;
+    dim3 grid((a.W + kFinTW - 1) / kFinTW, (a.H + kFinTH - 1) / kFinTH, nframes * 3);
     COUNT_LAUNCH();
-    finalize_kernel<<<grid, block, 0, s>>>(a);
+    finalize_kernel<<<grid, 256, smem, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -337,10 +339,12 @@ cudaError_t launch_vaggregate(const VAggArgs &a, int nframes, cudaStream_t s)
 
 cudaError_t launch_vstack(const VStackArgs &a, int nframes, cudaStream_t s)
 {
-    dim3 block(256);
-    dim3 grid((a.W + 255) / 256, a.H * a.slots, nframes * 3);
+    const size_t smem = sizeof(float) * (size_t)finalize_smem_floats(a.B);
+    cudaError_t e;
+    if ((e = allow_smem(vstack_kernel, smem)) != cudaSuccess) return e;
+    dim3 grid((a.W + kFinTW - 1) / kFinTW, a.slots * ((a.H + kFinTH - 1) / kFinTH), nframes * 3);
     COUNT_LAUNCH();
-    vstack_kernel<<<grid, block, 0, s>>>(a);
+    vstack_kernel<<<grid, 256, smem, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--frames", type=int, default=NFR)
     ap.add_argument("--width", type=int, default=W)
     ap.add_argument("--height", type=int, default=H)
+    ap.add_argument("--workload", default="bm3d", choices=["bm3d", "vbm3d"],
+                    help="bm3d: the headline Basic+Final pipeline; vbm3d: the V-BM3D pipeline of YUV444 16-bit "
+                         "clips (VBasic -> VAggregate -> VFinal -> VAggregate), stacked and aggregated forms")
     return ap.parse_args()
 
 
@@ -518,10 +521,116 @@ def ours_arm(args):
         dist.destroy_process_group()
 
 
+def vbm3d_arm(args):
+    """V-BM3D on a YUV444 16-bit 1920x1080 clip of `frames` frames (default 15), sigma 15, radius 1,
+    ps_num 2, ps_range 4: VBasic -> VAggregate -> VFinal(ref) -> VAggregate through the C ABI on
+    device-resident frames (the stacked drop-in chain), and the same chain with aggregate=1 (no
+    stacked clip).  Prints one JSON line; not the headline metric."""
+    import numpy as np
+    import torch
+    from bm3d_b200 import _capi as capi
+    from bm3d_b200 import synth
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    L = capi.lib()
+    F = args.frames if args.frames != NFR else 15
+    Wd, Hd, sig, r = args.width, args.height, 15.0, 1
+    nz, clean = synth.motion_frames(3, F, Hd, Wd, sig, planes=3)
+    yuv = np.stack([np.stack([synth.to_u16(np.clip(nz[f, c], 0, 1)) for c in range(3)]) for f in range(F)])
+    # 16-bit samples travel as int16 tensors (same bytes; torch's uint16 support is partial)
+    d_in = torch.from_numpy(np.ascontiguousarray(yuv).view(np.int16)).cuda()
+    stream = torch.cuda.Stream()
+    vi = capi.VideoInfo(capi.YUV, capi.INTEGER, 16, 0, 0, Wd, Hd, F)
+    common = {"sigma": sig, "radius": r}
+    D = capi.MEM_DEVICE
+
+    def planes(n, h, dt):
+        return [[torch.empty((h, Wd), dtype=dt, device="cuda") for _ in range(3)] for _ in range(n)]
+
+    _, a_in = make_frames(capi, [[d_in[k, p] for p in range(3)] for k in range(F)], D)
+    # stacked chain
+    vb = Stage(L, "VBasic", dict(common, input=vi, ps_num=2, ps_range=4), None)
+    ag1 = Stage(L, "VAggregate", {"input": vb.info, "radius": r}, None)
+    vf = Stage(L, "VFinal", dict(common, input=vi, ref=ag1.info), None)
+    ag2 = Stage(L, "VAggregate", {"input": vf.info, "radius": r}, None)
+    st_h = Hd * (2 * r + 1) * 2
+    f_vb, f_ag1 = planes(F, st_h, torch.float32), planes(F, Hd, torch.int16)
+    f_vf, f_ag2 = planes(F, st_h, torch.float32), planes(F, Hd, torch.int16)
+    _, a_vb = make_frames(capi, f_vb, D)
+    _, a_ag1 = make_frames(capi, f_ag1, D)
+    _, a_vf = make_frames(capi, f_vf, D)
+    _, a_ag2 = make_frames(capi, f_ag2, D)
+    # aggregated chain
+    fb = Stage(L, "VBasic", dict(common, input=vi, ps_num=2, ps_range=4, aggregate=1), None)
+    ff = Stage(L, "VFinal", dict(common, input=vi, ref=fb.info, aggregate=1), None)
+    f_fb, f_ff = planes(F, Hd, torch.int16), planes(F, Hd, torch.int16)
+    _, a_fb = make_frames(capi, f_fb, D)
+    _, a_ff = make_frames(capi, f_ff, D)
+    for st in (vb, ag1, vf, ag2, fb, ff):
+        L.bm3d_set_stream(st.h, C.c_void_p(stream.cuda_stream))
+
+    def call(st, src, ref, dst):
+        if L.bm3d_get_frames_async(st.h, 0, F, src, ref, dst) != 0:
+            raise RuntimeError(capi.last_error())
+
+    def stacked():
+        call(vb, a_in, None, a_vb)
+        call(ag1, a_vb, None, a_ag1)
+        call(vf, a_in, a_ag1, a_vf)
+        call(ag2, a_vf, None, a_ag2)
+
+    def fused():
+        call(fb, a_in, None, a_fb)
+        call(ff, a_in, a_fb, a_ff)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        tot = 0.0
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+            fn()
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / args.steps
+
+    clocks = Clocks(local)
+    clocks.start()
+    ms_st = timed(stacked)
+    ms_fu = timed(fused)
+    clk = clocks.stop()
+    out_st = torch.stack([torch.stack(f) for f in f_ag2]).cpu().numpy().view(np.uint16).astype(np.int64)
+    out_fu = torch.stack([torch.stack(f) for f in f_ff]).cpu().numpy().view(np.uint16).astype(np.int64)
+
+    def psnr16(o):
+        return 10 * np.log10(65535.0 ** 2 / np.mean((o - np.clip(np.round(clean * 65535.0), 0, 65535)) ** 2))
+
+    mpix = lambda ms: F * Wd * Hd / (ms * 1e-3) / 1e6
+    line = {"metric": "1080p V-BM3D Mpix/s (VBasic -> VAggregate -> VFinal -> VAggregate, YUV444 16-bit, radius 1)",
+            "value": round(mpix(ms_st), 3), "unit": "Mpix/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_st, 3), "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"YUV444 u16 {Wd}x{Hd} x{F} frames, translating scene, sigma 15", "radius": r,
+                       "ps_num": 2, "ps_range": 4},
+            "aggregated": {"value": round(mpix(ms_fu), 3), "ms_per_step": round(ms_fu, 3),
+                           "max_lsb_vs_stacked": int(np.abs(out_st - out_fu).max())},
+            "psnr_db": {"input": round(float(psnr16(yuv.astype(np.int64))), 3), "stacked": round(float(psnr16(out_st)), 3),
+                        "aggregated": round(float(psnr16(out_fu)), 3)},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload == "vbm3d":
+        vbm3d_arm(args)
     else:
         ours_arm(args)
 

@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
 {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ __align__(8) uint64_t mdrain;    // drains the products before the time-out path frees
     __shared__ uint32_t tslot;
     __shared__ float red[3][kBmtRefs];          // [1] candidate norm maxima, [2] window sums
     __shared__ float wlo[kBmtRefs], whi[kBmtRefs];
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
     float *rsq = reinterpret_cast<float *>(sm + L.offRsq);   // row sums of squares (centred)
 
     if (warp == 0) tc::tmem_alloc(&tslot, 256);
-    if (tid < 2) tc::mbar_init(&mbar[tid], 1);
+    if (tid < 3) tc::mbar_init(tid < 2 ? &mbar[tid] : &mdrain, 1);
     if (tid == 0) fail_flag = 0;
     if (tid < kBmtRefs) {
         int i = -1, l = 0, nc = 0;
@@ -291,8 +292,17 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
         tc::fence_after_sync();
         if (tid == 0 && ok && ph + 1 < nphases) issue(ph + 1);
     }
+    // After a timed-out wait, products may still be writing tensor memory: one more commit, which
+    // arrives once every product the issuing thread started has completed, is waited for (bounded)
+    // before the columns are released.
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) tc::mma_commit(&mdrain);
+        const bool drained = tc::mbar_wait_bounded(&mdrain, 0, kBmtWaitLimit);
+        tc::fence_after_sync();
+        if (tid == 0) atomicExch(&fail_flag, drained ? 1 : 2);
+        __syncthreads();
+    }
     if (warp == 0) tc::tmem_free(tm, 256);              // every load has completed (barrier above)
-    if (!ok) atomicExch(&fail_flag, 1);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) nbm = fmaxf(nbm, __shfl_xor_sync(0xffffffffu, nbm, o));
     if (lane == 0) red[1][warp] = nbm;

@@ -123,6 +123,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     constexpr int NT = WIENER ? 128 : 64;            // rows of the z-stage B operand
     extern __shared__ __align__(1024) unsigned char tsm[];
     __shared__ __align__(8) uint64_t mbar[NWG];
+    __shared__ __align__(8) uint64_t mdrain[NWG];   // drains a team's products on the time-out path
     __shared__ uint32_t tslot;
 
     const int wg = threadIdx.x / TEAM;
@@ -152,7 +153,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     if constexpr (Shp::kBoxes == 3)
         for (int i = t; i < Shp::kRegion; i += TEAM) Rg[i] = 0.0f;   // the aggregation box starts (and stays) zero
     if (warp == 0) tc::tmem_alloc(&tslot, Shp::kTmemCols);
-    if (t == 0) tc::mbar_init(&mbar[wg], 1);
+    if (t == 0) {
+        tc::mbar_init(&mbar[wg], 1);
+        tc::mbar_init(&mdrain[wg], 1);
+    }
     tc::fence_proxy_async_smem();
     tc::fence_before_sync();
     __syncthreads();
@@ -729,7 +733,15 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
         cur = nxt;
     }
     tc::cp_async_wait_all();                          // no box copy outlives the kernel
-    if (failed && t == 0) atomicExch(status, 1);
+    if (failed) {
+        // a timed-out wait leaves products possibly in flight: one more commit, which arrives once
+        // every product the issuing thread started has completed, is waited for (bounded) before
+        // the tensor memory is released; status 1 = time-out, 3 = the drain timed out as well
+        if (t == 0) tc::mma_commit(&mdrain[wg]);
+        const bool drained = tc::mbar_wait_bounded(&mdrain[wg], 0, kTcWaitLimit);
+        tc::fence_after_sync();
+        if (t == 0) atomicOr(status, drained ? 1 : 3);
+    }
     if (!WIENER && a.tc_stats && n_recheck) {
         atomicAdd(a.tc_stats, n_recheck);
         atomicAdd(a.tc_stats + 1, n_changed);

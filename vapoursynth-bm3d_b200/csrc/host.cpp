@@ -982,7 +982,8 @@ public:
         if (!tc_status.p) return;
         int st = 0;
         CU(cudaMemcpy(&st, tc_status.p, sizeof(int), cudaMemcpyDeviceToHost));
-        if (st) throw std::runtime_error(err("tensor-core collaborative filter timed out"));
+        if (st) throw std::runtime_error(err(st & 2 ? "tensor-core collaborative filter timed out (products still in flight after the drain wait)"
+                                                   : "tensor-core collaborative filter timed out"));
     }
 
     // float workspace conversion of one input frame set into plane slot `slot`

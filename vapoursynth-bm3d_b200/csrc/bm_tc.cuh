@@ -430,6 +430,68 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
                         done = true;
                     }
                 }
+            } else {
+                // a band too wide for registers: the exact distances of the band overwrite its
+                // estimates, the rest is marked invalid (it lies above the cut), and the (K + 1)
+                // smallest come out as in the plain selection: each lane's best two, the cut at
+                // the (K + 1)-th of their union, everything under it sorted.  Equal keys in the
+                // list or at the cut still take the exact path below.
+                int nval = 0, nbelow = 0;
+                uint64_t c1 = ~0ull, c2 = ~0ull;
+                for (int c0 = 0; c0 < ctot; c0 += 32) {
+                    const int c = c0 + ((lane + 7 * (c0 >> 5)) & 31);
+                    if (c >= ctot) continue;
+                    float d = 3.0e38f;
+                    if (sd[c] - mg <= bnd) d = exact_of((uint32_t)c);
+                    sd[c] = d;
+                    if (dist_valid(d, a.thSSE)) {
+                        ++nval;
+                        nbelow += d <= bnd;
+                        const uint64_t v = compose(d, (uint32_t)c);
+                        if (v < c1) { c2 = c1; c1 = v; } else if (v < c2) { c2 = v; }
+                    }
+                }
+                nval = warp_sum(nval);
+                nbelow = warp_sum(nbelow);
+                __syncwarp();
+                if (complete || nbelow > K) {
+                    uint64_t w2[2] = {c1, c2};
+                    warp_bitonic_u64<2>(w2);
+                    const int nout = min(nval, K);
+                    // every valid one when at most K + 1, else the cut at the (K + 1)-th of the union
+                    const uint64_t T = nval <= K + 1 ? ~0ull : __shfl_sync(0xffffffffu, w2[0], K);
+                    int m = 0;
+                    for (int c0 = 0; c0 < ctot; c0 += 32) {
+                        const int c = c0 + lane;
+                        const bool in = c < ctot && dist_valid(sd[c], a.thSSE) && compose(sd[c], (uint32_t)c) <= T;
+                        const unsigned msk = __ballot_sync(0xffffffffu, in);
+                        if (in && m + __popc(msk & lt) < 64) list[m + __popc(msk & lt)] = (uint32_t)c;
+                        m += __popc(msk);
+                    }
+                    __syncwarp();
+                    if (m <= 64) {
+                        uint64_t v[2] = {~0ull, ~0ull};
+                        if (lane < m) v[0] = compose(sd[list[lane]], list[lane]);
+                        if (lane + 32 < m) v[1] = compose(sd[list[lane + 32]], list[lane + 32]);
+                        warp_bitonic_u64<2>(v);
+                        const float key = lane <= nout && lane < nval ? dist_to_key(__uint_as_float((uint32_t)(v[0] >> 32)), a.distMul) : 0.0f;
+                        const float prev = __shfl_up_sync(0xffffffffu, key, 1);
+                        const bool bad = lane >= 1 && lane <= nout && lane < nval && !(prev < key);
+                        if (!__any_sync(0xffffffffu, bad)) {
+                            if (lane == 0) {
+                                a.out_pos[ob * G] = ref_pos;
+                                if (a.out_key) a.out_key[ob * G] = 0.0f;
+                                a.out_n[ob] = 1 + nout;
+                            }
+                            if (lane < nout) {
+                                a.out_pos[ob * G + 1 + lane] = pos_of((uint32_t)v[0]);
+                                if (a.out_key) a.out_key[ob * G + 1 + lane] = key;
+                            }
+                            done = true;
+                        }
+                    }
+                }
+                __syncwarp();
             }
         }
         if (!done) {

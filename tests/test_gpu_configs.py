@@ -9,7 +9,7 @@ drop-in has to reproduce.
   -> VAggregate, within 1 LSB; VBasic match lists of the middle frame index-identical.
 * 8-bit input, limited-range input (_Range = 0: chroma without clip, output rounding +0.5),
   integer RGB through Basic's internal OPP path, RGB2OPP / OPP2RGB with sample = 0, the 'vn'
-  Final (block size 11, generic filter kernel) and group_size 64.
+  Final (block size 11, generic filter kernel), group_size 64 / 128, bm_step / ps_step 2.
 
 Every test prints the tie events and hard-threshold flip counts of the oracle next to the GPU's
 exact tie-path block count (run pytest with -s to see them).
@@ -229,19 +229,37 @@ def test_vn_final_block11(orc):
     assert np.abs(gf - of).max() <= TOL
 
 
+@pytest.mark.parametrize("G", [64, 128])
 @pytest.mark.parametrize("wiener", [0, 1])
-def test_group_size_64(orc, wiener):
+def test_large_group_sizes(orc, wiener, G):
     nz, _ = synth.gray_frames(16, 1, 64, 72, 10.0)
-    pb = orc.default_params(0, False, "np", 10.0, width=72, height=64, group_size=64)
+    pb = orc.default_params(0, False, "np", 10.0, width=72, height=64, group_size=G)
     ob = orc.bm3d(pb, nz)
     if not wiener:
-        node = core.bm3d.Basic(source(nz, "GRAY"), profile="np", group_size=64)
+        node = core.bm3d.Basic(source(nz, "GRAY"), profile="np", group_size=G)
         g = node.numpy()
-        lists_equal(node, 0, orc.bm3d_matches(pb, nz[0, 0]), 64)
+        lists_equal(node, 0, orc.bm3d_matches(pb, nz[0, 0]), G)
         assert np.abs(g - ob).max() <= TOL
     else:
-        pf = orc.default_params(1, False, "np", 10.0, width=72, height=64, group_size=64)
-        node = core.bm3d.Final(source(nz, "GRAY"), source(ob, "GRAY"), profile="np", group_size=64)
+        pf = orc.default_params(1, False, "np", 10.0, width=72, height=64, group_size=G)
+        node = core.bm3d.Final(source(nz, "GRAY"), source(ob, "GRAY"), profile="np", group_size=G)
         g = node.numpy()
-        lists_equal(node, 0, orc.bm3d_matches(pf, ob[0, 0]), 64)
+        lists_equal(node, 0, orc.bm3d_matches(pf, ob[0, 0]), G)
         assert np.abs(g - orc.bm3d(pf, nz, ob)).max() <= TOL
+
+
+def test_search_steps_above_one(orc):
+    """bm_step = 2 (range-form lattice) and ps_step = 2 (predictive windows) outputs."""
+    nz, _ = synth.gray_frames(18, 1, 72, 96, 12.0)
+    pb = orc.default_params(0, False, "lc", 12.0, width=96, height=72, bm_step=2)
+    node = core.bm3d.Basic(source(nz, "GRAY"), profile="lc", sigma=12.0, bm_step=2)
+    g = node.numpy()
+    lists_equal(node, 0, orc.bm3d_matches(pb, nz[0, 0]), pb.G)
+    assert np.abs(g - orc.bm3d(pb, nz)).max() <= TOL
+    mz, _ = synth.motion_frames(19, 4, 40, 56, 12.0, planes=1)
+    clip = mz.astype(np.float32)
+    pv = orc.default_params(0, True, "lc", 12.0, width=56, height=40, ps_step=2, bm_step=2)
+    vb = core.bm3d.VBasic(source(clip, "GRAY"), profile="lc", sigma=12.0, ps_step=2, bm_step=2)
+    agg = core.bm3d.VAggregate(vb, radius=pv.radius, sample=1).numpy()
+    o_agg = orc.vaggregate(pv.radius, orc.vbm3d(pv, clip), process=(1, 0, 0))
+    assert np.abs(agg[:, 0] - o_agg[:, 0]).max() <= TOL

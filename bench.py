@@ -430,11 +430,17 @@ def ours_arm(args):
             for k2 in range(16):
                 hits += ((la[1][:, k] == ll[1][:, k2]) & (la[2][:, k] == ll[2][:, k2]) & (k < la[0]) & (k2 < ll[0]))
         recall_l = float(np.mean(hits / la[0]))
-    tcfb = {}
+    tcfb, lcut, rchk = {}, {}, {}
     for name, st in (("basic", pipes["tf32"].basic), ("final", pipes["tf32"].final)):
         fb, to = C.c_int64(0), C.c_int64(0)
         L.bm3d_debug_bm_tc_counts(st.h, C.byref(fb), C.byref(to))
         tcfb[name] = (int(fb.value), int(to.value))
+        # learned form: reference blocks whose proposal cut needed the exact radix selection
+        L.bm3d_debug_bm_tc_counts(getattr(pipes["learned"], name).h, C.byref(fb), C.byref(to))
+        lcut[name] = int(fb.value)
+    rc, ch = C.c_int64(0), C.c_int64(0)
+    L.bm3d_debug_threshold_rechecks(pipes["tf32"].basic.h, C.byref(rc), C.byref(ch))
+    rchk = {"recomputed": int(rc.value), "changed": int(ch.value)}
     bm_b, dct_b, _ = algorithmic_work(Wd, Hd, F, 4, 16, nb_mean, False)
     bm_f, dct_f, _ = algorithmic_work(Wd, Hd, F, 3, 32, nf_mean, True)
     stage = R["stage"]
@@ -502,7 +508,8 @@ def ours_arm(args):
                        "final_mean_n": round(nf_mean, 3), "final_full_fraction": round(nf_full, 4),
                        "basic_exact_tie_blocks": int(L.bm3d_debug_slow_blocks(pipe.basic.h)),
                        "final_exact_tie_blocks": int(L.bm3d_debug_slow_blocks(pipe.final.h))},
-            "learned_block_matching": {"basic_list_recall_vs_exhaustive": recall_l},
+            "learned_block_matching": {"basic_list_recall_vs_exhaustive": recall_l, "exact_cut_blocks": lcut},
+            "tc_threshold_recheck_basic": rchk,
             "tc_block_matching": {"basic_list_agreement_vs_fp32": agree,
                                   "exact_fallback_blocks": {k: v[0] for k, v in tcfb.items()},
                                   "timeouts": {k: v[1] for k, v in tcfb.items()}},

@@ -5,6 +5,8 @@ groups as tf32 matrix products, so its output differs slightly (hard-threshold d
 the threshold can flip).  Bars: PSNR against the clean frames within 0.05 dB of the plain path's;
 RMS deviation from the plain output below 10 % of the noise level, maximum below the noise level.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -88,30 +90,32 @@ def flips(node_tc, node_plain, k):
 
 
 @pytest.mark.parametrize("sigma", [5.0, 10.0, 30.0])
-def test_hard_threshold_flips_counted(sigma):
+def test_hard_threshold_flips_counted(orc, sigma):
     """Hard-threshold decisions of the precision form against the plain path, on the same match
-    lists (the tensor-core matching is exact): without the near-threshold recheck the tf32
-    coefficients flip some decisions; with it every coefficient within the band is recomputed in
-    fp32 from the pixels and no decision differs."""
+    lists (the tensor-core matching is exact), for a sweep of the recheck band.  Without the
+    recheck the tf32 coefficients flip some decisions; with it every coefficient within the band
+    is recomputed from the pixels in double precision, so the decisions left differing from the
+    plain path are those the plain FP32 transform itself takes against exact arithmetic (the
+    oracle counts them on the same frames)."""
     nz, _ = synth.gray_frames(55, 2, 540, 960, sigma)
     clip = source(nz, "GRAY")
     plain = core.bm3d.Basic(clip, profile="np", sigma=sigma)
     plain.numpy()
-    raw = core.bm3d.Basic(clip, profile="np", sigma=sigma, precision="tf32")
-    raw.set_recheck_band(0.0)
-    raw.numpy()
     tc = core.bm3d.Basic(clip, profile="np", sigma=sigma, precision="tf32")
-    tc.numpy()
-    f_raw = sum(flips(raw, plain, k)[0] for k in range(2))
-    f_tc, dec = 0, 0
-    for k in range(2):
-        f, d = flips(tc, plain, k)
-        f_tc += f
-    rechecked, changed = tc.threshold_rechecks()
+    res = {}
+    for band in (0.0, 1.0 / 4096, 1.0 / 1024, 1.0 / 256, 1.0 / 64):
+        tc.set_recheck_band(band)
+        tc.compute(0, 2)
+        res[band] = (sum(flips(tc, plain, k)[0] for k in range(2)),) + tc.threshold_rechecks()
+    pb = orc.default_params(0, False, "np", sigma, width=960, height=540)
+    _, st = orc.bm3d(pb, nz, threads=max(1, os.cpu_count() or 1), stats=True)
     kept = sum(int(plain.retained_counts(k)[0].sum()) for k in range(2))
-    print(f"sigma {sigma}: retained {kept}, flips without recheck {f_raw}, with recheck {f_tc}; "
-          f"recomputed {rechecked}, changed {changed}")
-    assert f_tc == 0
+    print(f"\nsigma {sigma}: decisions {st['coefficients']}, retained {kept}, plain FP32 vs FP64 flips "
+          f"(oracle) {st['flips_vs_fp64']}; band -> (flips vs plain, recomputed, changed): "
+          + ", ".join(f"1/{int(round(1 / b)) if b else 0}: {v}" for b, v in res.items()))
+    f_raw, f_tc = res[0.0][0], res[1.0 / 256][0]
+    assert f_raw > 0
+    assert f_tc <= 2 * st["flips_vs_fp64"] + 4
 
 
 def list_agreement(a, b, k, G):
@@ -154,4 +158,8 @@ def test_precision_form_2160p(sigma):
           f"vs FP64 basic plain [{stat(res['fp32']['eb'])}] tf32 [{stat(res['tf32']['eb'])}], "
           f"final plain [{stat(res['fp32']['ef'])}] tf32 [{stat(res['tf32']['ef'])}]")
     assert agree_b == 1.0 and agree_f == 1.0
-    assert abs(d_final) <= PSNR_TOL_DB and fl == 0
+    assert abs(d_final) <= PSNR_TOL_DB
+    # decisions left differing from the plain path: of the order of the plain path's own FP32
+    # flips against exact arithmetic (about 1e-8 of the decisions at 1080p)
+    decisions = 4 * res["fp32"]["b"].retained_counts(0).shape[1] * 16 * 64
+    assert fl <= 1e-7 * decisions

@@ -350,9 +350,9 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     };
     const int pfirst = next_plane(0);
     const long long tstride = (long long)gridDim.x * NWG;
-    // fp32 tables after the tensor-core image: C8[u][y] = 2 cos(pi (2y + 1) u / 16), then the
+    // fp64 tables after the tensor-core image: C8[u][y] = 2 cos(pi (2y + 1) u / 16), then the
     // z matrix Dz[kz][b] = 2 cos(pi (2b + 1) kz / 2G) (hard-threshold recheck and block means)
-    const float *xtab = reinterpret_cast<const float *>(reinterpret_cast<const unsigned char *>(tables) + Lay::kTableBytes);
+    const double *xtab = reinterpret_cast<const double *>(reinterpret_cast<const unsigned char *>(tables) + Lay::kTableBytes);
     unsigned long long n_recheck = 0, n_changed = 0;
 
     bool failed = false;
@@ -517,9 +517,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             uint64_t flags = 0;                        // columns (relative to cb) to recompute
             if constexpr (!WIENER) {
                 const int gl = (lane / G) * G;         // lane of the group's first block
+                double dz = 0.0;
 #pragma unroll 4
-                for (int b = 0; b < G; ++b) dcz = fmaf(__ldg(xtab + 64 + j * G + b), __shfl_sync(0xffffffffu, my_mu, gl + b), dcz);
-                dcz *= 256.0f;
+                for (int b = 0; b < G; ++b) dz = fma(__ldg(xtab + 64 + j * G + b), (double)__shfl_sync(0xffffffffu, my_mu, gl + b), dz);
+                dcz = (float)(256.0 * dz);
             }
             const float band = WIENER ? 0.0f : a.recheck_band;
 #pragma unroll
@@ -557,9 +558,9 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 for (int e = 0; e < 32; ++e) *reinterpret_cast<float *>(D + tc::sw128_offset(cb + c0 + e, r, 64)) = z[e];
             }
             if constexpr (!WIENER) {
-                // coefficients near their threshold: the exact fp32 value from the pixels decides
-                // sum_b Dz[kz][b] sum_y C8[u][y] sum_x C8[v][x] x_b(y, x); the warp computes one
-                // at a time, lane = (pixel row y, every fourth block)
+                // coefficients near their threshold: the value from the pixels in double precision
+                // decides, sum_b Dz[kz][b] sum_y C8[u][y] sum_x C8[v][x] x_b(y, x); the warp
+                // computes one at a time, lane = (pixel row y, every fourth block)
                 while (true) {
                     const unsigned anyf = __ballot_sync(0xffffffffu, flags != 0ull);
                     if (!anyf) break;
@@ -568,7 +569,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     const int c = cb + __ffsll((long long)lf) - 1;
                     const int u = c >> 3, v = c & 7, kz = ldr % G, gl = (ldr / G) * G;
                     const int yy = lane & 7;
-                    float sum = 0.0f;
+                    double sum = 0.0;
 #pragma unroll
                     for (int k = 0; k < G / 4; ++k) {
                         const int bb = (lane >> 3) + 4 * k;
@@ -585,10 +586,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                             pitch = a.ld;
                         }
                         (void)pitch;
-                        float rs = 0.0f;
+                        double rs = 0.0;
 #pragma unroll
-                        for (int x = 0; x < 8; ++x) rs = fmaf(__ldg(xtab + v * 8 + x), px[x], rs);
-                        sum = fmaf(__ldg(xtab + 64 + kz * G + bb) * __ldg(xtab + u * 8 + yy), rs, sum);
+                        for (int x = 0; x < 8; ++x) rs = fma(__ldg(xtab + v * 8 + x), (double)px[x], rs);
+                        sum = fma(__ldg(xtab + 64 + kz * G + bb) * __ldg(xtab + u * 8 + yy), rs, sum);
                     }
 #pragma unroll
                     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -596,8 +597,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         flags &= flags - 1;
                         float *sv = reinterpret_cast<float *>(D + tc::sw128_offset(c, r, 64));
                         const float th = thr[((c & 7) == 0) + ((c >> 3) == 0)];
-                        const bool keep_old = *sv != 0.0f, keep_new = fabsf(sum) > th;
-                        *sv = keep_new ? sum : 0.0f;
+                        const bool keep_old = *sv != 0.0f, keep_new = fabs(sum) > (double)th;
+                        *sv = keep_new ? (float)sum : 0.0f;
                         acc += (keep_new ? 1.0f : 0.0f) - (keep_old ? 1.0f : 0.0f);
                         ++n_recheck;
                         n_changed += keep_new != keep_old;

@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -704,10 +705,10 @@ public:
 // Learned block-matching proposal: device buffers and the descriptor pass
 
 // Precision form, hard threshold: coefficients whose tensor-core value lies within this fraction
-// of their threshold are recomputed in fp32 before the keep / zero decision.  The tf32 products
-// of mean-free blocks stay well inside it (the test suite counts the decisions that still differ
-// from the plain path's at 1080p and 2160p).
-constexpr float kRecheckBand = 1.0f / 64.0f;
+// of their threshold are recomputed from the pixels in double precision before the keep / zero
+// decision.  The tf32 products of mean-free blocks stay inside it (the test suite sweeps the
+// band and counts the decisions that still differ from the plain path's).
+constexpr float kRecheckBand = 1.0f / 256.0f;
 
 // proposals per reference block that the learned form re-ranks exactly (of about 1,089 at range 16)
 constexpr int kLearnedProposals = 96;
@@ -954,15 +955,16 @@ public:
         if (tc && cf_tc_supported(para.B, para.G)) {
             std::vector<unsigned char> img;
             cf_tc_tables(para.G, img);
-            // fp32 tables of the hard-threshold recheck after the image: C8[u][y], Dz[kz][b]
-            std::vector<float> xt;
+            // fp64 tables of the hard-threshold recheck after the image: C8[u][y], Dz[kz][b]
+            std::vector<double> xt;
+            const double pi = 3.14159265358979323846;
             for (int u = 0; u < 8; ++u)
-                for (int y = 0; y < 8; ++y) xt.push_back(cos2((long)(2 * y + 1) * u, 16L));
+                for (int y = 0; y < 8; ++y) xt.push_back(2.0 * std::cos(pi * (2 * y + 1) * u / 16.0));
             for (int kz = 0; kz < para.G; ++kz)
-                for (int b = 0; b < para.G; ++b) xt.push_back(cos2((long)(2 * b + 1) * kz, 2L * para.G));
+                for (int b = 0; b < para.G; ++b) xt.push_back(2.0 * std::cos(pi * (2 * b + 1) * kz / (2.0 * para.G)));
             const size_t base = img.size();
-            img.resize(base + xt.size() * sizeof(float));
-            std::memcpy(img.data() + base, xt.data(), xt.size() * sizeof(float));
+            img.resize(base + xt.size() * sizeof(double));
+            std::memcpy(img.data() + base, xt.data(), xt.size() * sizeof(double));
             CU(cudaMemcpy(tc_tab.get(img.size()), img.data(), img.size(), cudaMemcpyHostToDevice));
             CU(cudaMemset(tc_status.get(sizeof(int)), 0, sizeof(int)));
         }

@@ -113,7 +113,7 @@ def test_hard_threshold_flips_counted(orc, sigma):
     print(f"\nsigma {sigma}: decisions {st['coefficients']}, retained {kept}, plain FP32 vs FP64 flips "
           f"(oracle) {st['flips_vs_fp64']}; band -> (flips vs plain, recomputed, changed): "
           + ", ".join(f"1/{int(round(1 / b)) if b else 0}: {v}" for b, v in res.items()))
-    f_raw, f_tc = res[0.0][0], res[1.0 / 256][0]
+    f_raw, f_tc = res[0.0][0], res[1.0 / 64][0]
     assert f_raw > 0
     assert f_tc <= 2 * st["flips_vs_fp64"] + 4
 

@@ -517,12 +517,18 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             uint64_t flags = 0;                        // columns (relative to cb) to recompute
             if constexpr (!WIENER) {
                 const int gl = (lane / G) * G;         // lane of the group's first block
-                double dz = 0.0;
 #pragma unroll 4
-                for (int b = 0; b < G; ++b) dz = fma(__ldg(xtab + 64 + j * G + b), (double)__shfl_sync(0xffffffffu, my_mu, gl + b), dz);
-                dcz = (float)(256.0 * dz);
+                for (int b = 0; b < G; ++b) dcz = fmaf((float)__ldg(xtab + 64 + j * G + b), __shfl_sync(0xffffffffu, my_mu, gl + b), dcz);
+                dcz *= 256.0f;
             }
-            const float band = WIENER ? 0.0f : a.recheck_band;
+            // the recheck interval [lo, hi] of |c| around each of the three threshold classes
+            float tlo[3], thi[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float band = WIENER ? 0.0f : a.recheck_band;
+                tlo[k] = mine ? thr[k] * (1.0f - band) : 3.0e38f;
+                thi[k] = thr[k] * (1.0f + band);
+            }
 #pragma unroll
             for (int c0 = 0; c0 < NC; c0 += 32) {
                 float z[32];
@@ -547,9 +553,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
 #pragma unroll
                     for (int e = 0; e < 32; ++e) {
                         const int c = cb + c0 + e;
-                        const float th = thr[((c & 7) == 0) + ((c >> 3) == 0)];
-                        const bool keep = fabsf(z[e]) > th;
-                        if (mine && fabsf(fabsf(z[e]) - th) <= band * th) flags |= 1ull << (c0 + e);
+                        const int k = ((c & 7) == 0) + ((c >> 3) == 0);
+                        const float az = fabsf(z[e]);
+                        const bool keep = az > thr[k];
+                        if (az >= tlo[k] && az <= thi[k]) flags |= 1ull << (c0 + e);
                         acc += keep ? 1.0f : 0.0f;
                         z[e] = keep ? z[e] : 0.0f;
                     }

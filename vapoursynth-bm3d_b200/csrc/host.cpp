@@ -706,9 +706,10 @@ public:
 
 // Precision form, hard threshold: coefficients whose tensor-core value lies within this fraction
 // of their threshold are recomputed from the pixels in double precision before the keep / zero
-// decision.  The tf32 products of mean-free blocks stay inside it (the test suite sweeps the
-// band and counts the decisions that still differ from the plain path's).
-constexpr float kRecheckBand = 1.0f / 256.0f;
+// decision.  The tf32 products of mean-free blocks stay inside it: with this band the decisions
+// left differing from the plain path's are the plain FP32 transform's own flips against exact
+// arithmetic (the test suite sweeps the band and counts them against the oracle's).
+constexpr float kRecheckBand = 1.0f / 64.0f;
 
 // proposals per reference block that the learned form re-ranks exactly (of about 1,089 at range 16)
 constexpr int kLearnedProposals = 96;

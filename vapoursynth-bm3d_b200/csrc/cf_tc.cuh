@@ -373,10 +373,12 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             if (!a.process[p]) continue;
             const GroupLoc L = locate(a, p, g0, pk);
             const bool last = next_plane(p + 1) >= 3;
-            // hard threshold: every block enters the products with its mean removed, so that the
-            // tf32 rounding scales with the block's detail, not its level; the means' own
-            // transform (the (0, 0) coefficients) is added back exactly in fp32 before the threshold
-            float my_mu = 0.0f;
+            // Every block enters the products with its mean removed (source and, for the Wiener
+            // filter, reference), so that the tf32 rounding scales with the block's detail, not
+            // its level; the means' own transform (the (0, 0) coefficients of every z frequency)
+            // is added back in fp32 before the shrinkage.  Likewise the shrunk (0, 0) coefficients
+            // leave the inverse products and come back as one fp32 constant per block.
+            float my_mu = 0.0f, my_mur = 0.0f;
             // 1. gather (rows of foreign or partial groups are zero), one block per warp step
             if (region) {
                 if constexpr (Shp::kBoxes == 3) {
@@ -395,12 +397,25 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                             u0 = Br[(by + ry) * rp + bx + cx];
                             u1 = Br[(by + ry + 4) * rp + bx + cx];
                         }
+                        {
+                            const float ms = block_mean(v0, v1), mr = block_mean(u0, u1);
+                            v0 -= ms;
+                            v1 -= ms;
+                            u0 -= mr;
+                            u1 -= mr;
+                            if (lane == 0) {
+                                part[b0 + i] = ms;
+                                part[128 + b0 + i] = mr;
+                            }
+                        }
                         *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128)) = v0;
                         *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
                         *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128)) = u0;
                         *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane + 32, 128)) = u1;
                     }
                     tc::wg_sync(bar_id, TEAM);
+                    my_mu = part[r];
+                    my_mur = part[128 + r];
                     // the next plane's boxes load while this plane is filtered
                     if (!last) load_boxes(cur, next_plane(p + 1));
                 } else {
@@ -425,19 +440,22 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                                 v0 = Rg[(by + ry) * rp + bx + cx];
                                 v1 = Rg[(by + ry + 4) * rp + bx + cx];
                             }
-                            if constexpr (!WIENER) {
+                            {
                                 const float mu = block_mean(v0, v1);
                                 v0 -= mu;
                                 v1 -= mu;
                                 if (lane == i) my_mu = mu;
-                                if constexpr (SPLIT == 2) if (lane == 0) part[b0 + i] = mu;
+                                if constexpr (SPLIT >= 2) if (lane == 0) part[(pass == 0 ? 128 : 0) + b0 + i] = mu;
                             }
                             *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane, 128)) = v0;
                             *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
                         }
                         tc::wg_sync(bar_id, TEAM);
                     }
-                    if constexpr (!WIENER && SPLIT == 2) my_mu = part[r];
+                    if constexpr (SPLIT >= 2) {
+                        my_mu = part[r];
+                        if constexpr (WIENER) my_mur = part[128 + r];
+                    }
                 }
             } else {
                 const float *sp = L.src + (long long)L.y * a.ld + L.x;
@@ -467,21 +485,24 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     }
                 }
                 tc::cp_async_wait_all();
-                if constexpr (!WIENER) {
+                // each lane re-reads only the elements its own copies wrote
 #pragma unroll 4
-                    for (int i = half * NI; i < half * NI + NI; ++i) {
-                        float *d0 = reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128));
-                        float *d1 = reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128));
+                for (int i = half * NI; i < half * NI + NI; ++i) {
+#pragma unroll
+                    for (int op = 0; op < (WIENER ? 2 : 1); ++op) {
+                        float *d0 = reinterpret_cast<float *>(D + op * Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128));
+                        float *d1 = reinterpret_cast<float *>(D + op * Lay::kXBytes + tc::sw128_offset(b0 + i, lane + 32, 128));
                         const float mu = block_mean(*d0, *d1);
                         *d0 -= mu;
                         *d1 -= mu;
-                        if (lane == i) my_mu = mu;
-                        if constexpr (SPLIT == 2) if (lane == 0) part[b0 + i] = mu;
+                        if (op == 0 && lane == i) my_mu = mu;
+                        if constexpr (SPLIT >= 2) if (lane == 0) part[128 * op + b0 + i] = mu;
                     }
-                    if constexpr (SPLIT == 2) {
-                        tc::wg_sync(bar_id, TEAM);
-                        my_mu = part[r];
-                    }
+                }
+                if constexpr (SPLIT >= 2) {
+                    tc::wg_sync(bar_id, TEAM);
+                    my_mu = part[r];
+                    if constexpr (WIENER) my_mur = part[128 + r];
                 }
             }
             if (last) {
@@ -513,13 +534,18 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
 #pragma unroll
             for (int k = 0; k < 3; ++k) thr[k] = WIENER ? 0.0f : a.thr4[p][G - 1][(j == 0) + k];
             // (hard threshold) the exact z transform of the block means' (0, 0) coefficients 256 mu
-            float dcz = 0.0f;
+            float dcz = 0.0f, dczr = 0.0f;
             uint64_t flags = 0;                        // columns (relative to cb) to recompute
-            if constexpr (!WIENER) {
+            {
                 const int gl = (lane / G) * G;         // lane of the group's first block
 #pragma unroll 4
-                for (int b = 0; b < G; ++b) dcz = fmaf((float)__ldg(xtab + 64 + j * G + b), __shfl_sync(0xffffffffu, my_mu, gl + b), dcz);
+                for (int b = 0; b < G; ++b) {
+                    const float dzb = (float)__ldg(xtab + 64 + j * G + b);
+                    dcz = fmaf(dzb, __shfl_sync(0xffffffffu, my_mu, gl + b), dcz);
+                    if constexpr (WIENER) dczr = fmaf(dzb, __shfl_sync(0xffffffffu, my_mur, gl + b), dczr);
+                }
                 dcz *= 256.0f;
+                dczr *= 256.0f;
             }
             // the recheck interval [lo, hi] of |c| around each of the three threshold classes
             float tlo[3], thi[3];
@@ -539,6 +565,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     tc::tmem_ld16(tb + lrow + 64 + cb + c0, *reinterpret_cast<float (*)[16]>(rr));
                     tc::tmem_ld16(tb + lrow + 64 + cb + c0 + 16, *reinterpret_cast<float (*)[16]>(rr + 16));
                     tc::tmem_wait_ld();
+                    if (cb + c0 == 0) {
+                        z[0] += dcz;
+                        rr[0] += dczr;
+                    }
                     const float sg = a.wsig2[p][G - 1];
 #pragma unroll
                     for (int e = 0; e < 32; ++e) {
@@ -612,6 +642,13 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     }
                 }
             }
+            // the shrunk (0, 0) coefficient of this row leaves the inverse products
+            float s00 = 0.0f;
+            if (cb == 0) {
+                float *s0p = reinterpret_cast<float *>(D + tc::sw128_offset(0, r, 64));
+                s00 = *s0p;
+                *s0p = 0.0f;
+            }
 #pragma unroll
             for (int o = G / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             if constexpr (SPLIT == 2) {
@@ -631,6 +668,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             }
             const float numW = denW / a.amp[G - 1];
             publish();
+            // (the barriers of the two inverse waits below order this before the aggregation)
+            if constexpr (SPLIT >= 2) if (half == 0) part[r] = s00;
             // 6. inverse z, then inverse 2-D
             if (t == 0) {
                 z_stage(0, sZi, 64, ID64);
@@ -647,7 +686,20 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 float v[NC];
 #pragma unroll
                 for (int c0 = 0; c0 < NC; c0 += 16) tc::tmem_ld16(tb + lrow + 64 + cb + c0, *reinterpret_cast<float (*)[16]>(v + c0));
+                // the inverse of the (0, 0) coefficients: block j of the group gets
+                // sum_kz Ci[j][kz] S(kz, 0, 0), Ci[j][0] = 1, Ci[j][kz] = Dz[kz][j]
+                float dcb = 0.0f;
+                {
+                    const int gl = (lane / G) * G;
+#pragma unroll 4
+                    for (int kz = 0; kz < G; ++kz) {
+                        const float sk = SPLIT == 1 ? __shfl_sync(0xffffffffu, s00, gl + kz) : part[(r / G) * G + kz];
+                        dcb = fmaf(kz == 0 ? 1.0f : (float)__ldg(xtab + 64 + kz * G + j), sk, dcb);
+                    }
+                }
                 tc::tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < NC; ++c) v[c] += dcb;
 #pragma unroll
                 for (int c = 0; c < NC; c += 4)
                     *reinterpret_cast<float4 *>(D + tc::sw128_offset(r, cb + c, 128)) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);

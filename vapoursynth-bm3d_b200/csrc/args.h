@@ -31,9 +31,12 @@ BM3D_HD inline int bm_warp_floats(int cand_cap, int G, int B, bool generic)
 }
 // bm_learned_kernel: scores, then a 128-entry candidate list
 BM3D_HD inline int prop_warp_floats(int cand_cap) { return cand_cap + 128; }
+// per warp: sp, tmp (at least 128 entries: also the radix-selection histogram), sk, the
+// concatenated list (keys, positions), the per-frame selection, centres, heap, reference block
+BM3D_HD inline int vbm_tmp_cap(int sp_cap) { return sp_cap > 128 ? sp_cap : 128; }
 BM3D_HD inline int vbm_warp_floats(int sp_cap, int list_cap, int G, int ps_num, int B)
 {
-    return 3 * sp_cap + 4 * list_cap + 2 * G + ps_num + B * B;
+    return 2 * sp_cap + vbm_tmp_cap(sp_cap) + 4 * list_cap + 2 * G + ps_num + B * B;
 }
 
 // Precision-form block matching (bm_tc_kernel): at most kBmtRefs reference blocks per CTA and

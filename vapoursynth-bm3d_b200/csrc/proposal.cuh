@@ -439,54 +439,8 @@ __global__ void __launch_bounds__(256) bm_learned_kernel(BMArgs a, const __nv_bf
         // score and, of those equal to it, the first ones in scan order -- exactly the pr + 1
         // smallest (score, index) keys.
         if (lane == 0 && a.stats) atomicAdd(a.stats + 1, 1ull);
-        int *hist = reinterpret_cast<int *>(list);
-        uint32_t prefix = 0, pmask = 0;
         int rank = pr;
-        for (int pass = 0; pass < 5; ++pass) {
-            const int shift = pass < 4 ? 24 - 7 * pass : 0;
-            const uint32_t dmask = pass < 4 ? 127u : 7u;
-            for (int e = lane; e < 128; e += 32) hist[e] = 0;
-            __syncwarp();
-            for (int c = lane; c < ctot; c += 32) {
-                const uint32_t u = __float_as_uint(sd[c]);
-                if ((u & pmask) == prefix) atomicAdd(&hist[(u >> shift) & dmask], 1);
-            }
-            __syncwarp();
-            int h[4], tot = 0;
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                h[e] = hist[4 * lane + e];
-                tot += h[e];
-            }
-            int incl = tot;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            const int excl = incl - tot;
-            const bool mine_bin = rank >= excl && rank < incl;
-            int dsel = 0, before = 0;
-            if (mine_bin) {
-                int run = excl;
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    if (rank >= run && rank < run + h[e]) {
-                        dsel = 4 * lane + e;
-                        before = run;
-                    }
-                    run += h[e];
-                }
-            }
-            const unsigned owner = __ballot_sync(0xffffffffu, mine_bin);
-            const int src = __ffs(owner) - 1;
-            dsel = __shfl_sync(0xffffffffu, dsel, src);
-            before = __shfl_sync(0xffffffffu, before, src);
-            rank -= before;
-            prefix |= (uint32_t)dsel << shift;
-            pmask |= dmask << shift;
-            __syncwarp();
-        }
+        const uint32_t prefix = warp_radix_cut(sd, ctot, rank, reinterpret_cast<int *>(list));
         // prefix = the score of rank pr; rank = its position among the candidates of that score
         int cnt = 0, eq = 0;
         for (int c0 = 0; c0 < ctot; c0 += 32) {

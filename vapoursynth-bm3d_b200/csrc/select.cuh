@@ -139,4 +139,61 @@ __device__ __forceinline__ uint64_t compose(float positive_value, uint32_t idx)
     return ((uint64_t)__float_as_uint(positive_value) << 32) | idx;
 }
 
+// Warp-wide radix selection over n non-negative scores sc[0..n) (their bit patterns order like the
+// values): the score S of rank `rank` (0-based, rank < n) and how many entries equal to S come
+// before it in that order (returned in rank).  With them, the rank + 1 smallest (score, index)
+// pairs are every entry below S plus the first rank + 1 entries equal to S in index order.
+// Five passes of 7, 7, 7, 7 and 3 bits with a 128-bin histogram in hist (128 ints of shared
+// memory owned by the warp).
+__device__ __forceinline__ uint32_t warp_radix_cut(const float *sc, int n, int &rank, int *hist)
+{
+    const int lane = (int)(threadIdx.x & 31);
+    uint32_t prefix = 0, pmask = 0;
+    for (int pass = 0; pass < 5; ++pass) {
+        const int shift = pass < 4 ? 24 - 7 * pass : 0;
+        const uint32_t dmask = pass < 4 ? 127u : 7u;
+        for (int e = lane; e < 128; e += 32) hist[e] = 0;
+        __syncwarp();
+        for (int c = lane; c < n; c += 32) {
+            const uint32_t u = __float_as_uint(sc[c]);
+            if ((u & pmask) == prefix) atomicAdd(&hist[(u >> shift) & dmask], 1);
+        }
+        __syncwarp();
+        int h[4], tot = 0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            h[e] = hist[4 * lane + e];
+            tot += h[e];
+        }
+        int incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - tot;
+        const bool own = rank >= excl && rank < incl;
+        int dsel = 0, before = 0;
+        if (own) {
+            int run = excl;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                if (rank >= run && rank < run + h[e]) {
+                    dsel = 4 * lane + e;
+                    before = run;
+                }
+                run += h[e];
+            }
+        }
+        const int src = __ffs(__ballot_sync(0xffffffffu, own)) - 1;
+        dsel = __shfl_sync(0xffffffffu, dsel, src);
+        before = __shfl_sync(0xffffffffu, before, src);
+        rank -= before;
+        prefix |= (uint32_t)dsel << shift;
+        pmask |= dmask << shift;
+        __syncwarp();
+    }
+    return prefix;
+}
+
 }  // namespace bm3d

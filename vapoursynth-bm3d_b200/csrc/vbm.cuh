@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(128) vbm_predict_kernel(VBMArgs a)
     float *base = smem + (size_t)warp * per_warp;
     uint32_t *sp = reinterpret_cast<uint32_t *>(base);
     uint32_t *tmp = sp + a.sp_cap;
-    float *sk = reinterpret_cast<float *>(tmp + a.sp_cap);
+    float *sk = reinterpret_cast<float *>(tmp + vbm_tmp_cap(a.sp_cap));
     float *lk = sk + a.sp_cap;                                  // concatenated keys
     uint32_t *lp = reinterpret_cast<uint32_t *>(lk + a.list_cap); // concatenated positions (zyx)
     float *fk = reinterpret_cast<float *>(lp + a.list_cap);     // per-frame selection keys
@@ -259,7 +259,6 @@ __global__ void __launch_bounds__(128) vbm_predict_kernel(VBMArgs a)
                 // learned proposals: the nprop positions of smallest descriptor distance (ties by
                 // position order) get exact distances, the others are left out of this frame's list
                 const __nv_bfloat16 *dz = dsc + (long long)(wbase + fz) * a.desc_frame * kPropCh;
-                uint64_t mx = 0;
                 for (int c = lane; c < ns; c += 32) {
                     float dc[kPropCh];
                     load_desc(dz, (long long)unpack_y(sp[c]) * Wd + unpack_x(sp[c]), dc);
@@ -267,31 +266,28 @@ __global__ void __launch_bounds__(128) vbm_predict_kernel(VBMArgs a)
 #pragma unroll
                     for (int k = 0; k < kPropCh; ++k) sc = fmaf(da[k] - dc[k], da[k] - dc[k], sc);
                     sk[c] = sc;
-                    mx = max(mx, compose(sc, (uint32_t)c));
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-                __syncwarp();
-                // the nprop-th smallest (score, index) key by bisection: the keys are distinct
-                uint64_t lo = 0, hi = mx;
-                while (lo < hi) {
-                    const uint64_t mid = lo + ((hi - lo) >> 1);
-                    int cnt = 0;
-                    for (int c0 = 0; c0 < ns; c0 += 32) {
-                        const int c = c0 + lane;
-                        cnt += __popc(__ballot_sync(0xffffffffu, c < ns && compose(sk[c], (uint32_t)c) <= mid));
-                    }
-                    if (cnt >= a.nprop) hi = mid;
-                    else lo = mid + 1;
                 }
                 __syncwarp();
-                for (int c = lane; c < ns; c += 32) {
-                    float key = -1.0f;
-                    if (compose(sk[c], (uint32_t)c) <= hi) {
-                        const float d = ssd8_global(rb, plane + (long long)unpack_y(sp[c]) * a.ld + unpack_x(sp[c]), a.ld);
-                        key = dist_valid(d, a.thSSE) ? dist_to_key(d, a.distMul) : -1.0f;
+                // the nprop smallest (score, position index) by radix selection (tmp is free here)
+                int rank = a.nprop - 1;
+                const uint32_t cutv = warp_radix_cut(sk, ns, rank, reinterpret_cast<int *>(tmp));
+                const unsigned lt = (1u << lane) - 1u;
+                int eq = 0;
+                for (int c0 = 0; c0 < ns; c0 += 32) {
+                    const int c = c0 + lane;
+                    const uint32_t u = c < ns ? __float_as_uint(sk[c]) : 0xffffffffu;
+                    const bool isq = c < ns && u == cutv;
+                    const unsigned mq = __ballot_sync(0xffffffffu, isq);
+                    const bool in = c < ns && (u < cutv || (isq && eq + __popc(mq & lt) <= rank));
+                    eq += __popc(mq);
+                    if (c < ns) {
+                        float key = -1.0f;
+                        if (in) {
+                            const float d = ssd8_global(rb, plane + (long long)unpack_y(sp[c]) * a.ld + unpack_x(sp[c]), a.ld);
+                            key = dist_valid(d, a.thSSE) ? dist_to_key(d, a.distMul) : -1.0f;
+                        }
+                        sk[c] = key;
                     }
-                    sk[c] = key;
                 }
             } else {
                 for (int c = lane; c < ns; c += 32) {

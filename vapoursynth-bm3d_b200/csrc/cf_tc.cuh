@@ -385,33 +385,34 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     if (half == 0) rowtab[r].x = mine ? ((L.y - y0) << 16) | (L.x - x0) : -1;
                     tc::cp_async_wait_all();
                     tc::wg_sync(bar_id, TEAM);
-#pragma unroll 4
-                    for (int i = half * NI; i < half * NI + NI; ++i) {
-                        const int pq = rowtab[b0 + i].x;
-                        const bool mi = pq >= 0;
-                        const int by = pq >> 16, bx = pq & 0xffff;
-                        float v0 = 0.f, v1 = 0.f, u0 = 0.f, u1 = 0.f;
-                        if (mi) {
-                            v0 = Bs[(by + ry) * rp + bx + cx];
-                            v1 = Bs[(by + ry + 4) * rp + bx + cx];
-                            u0 = Br[(by + ry) * rp + bx + cx];
-                            u1 = Br[(by + ry + 4) * rp + bx + cx];
+                    // four block steps per round: their loads are issued before any store
+                    for (int i0 = half * NI; i0 < half * NI + NI; i0 += 4) {
+                        int pq[4];
+                        float v0[4], v1[4], u0[4], u1[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) pq[k] = rowtab[b0 + i0 + k].x;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const bool mi = pq[k] >= 0;
+                            const int o = mi ? ((pq[k] >> 16) + ry) * rp + (pq[k] & 0xffff) + cx : 0;
+                            v0[k] = mi ? Bs[o] : 0.f;
+                            v1[k] = mi ? Bs[o + 4 * rp] : 0.f;
+                            u0[k] = mi ? Br[o] : 0.f;
+                            u1[k] = mi ? Br[o + 4 * rp] : 0.f;
                         }
-                        {
-                            const float ms = block_mean(v0, v1), mr = block_mean(u0, u1);
-                            v0 -= ms;
-                            v1 -= ms;
-                            u0 -= mr;
-                            u1 -= mr;
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const int i = i0 + k;
+                            const float ms = block_mean(v0[k], v1[k]), mr = block_mean(u0[k], u1[k]);
                             if (lane == 0) {
                                 part[b0 + i] = ms;
                                 part[128 + b0 + i] = mr;
                             }
+                            *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128)) = v0[k] - ms;
+                            *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1[k] - ms;
+                            *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128)) = u0[k] - mr;
+                            *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane + 32, 128)) = u1[k] - mr;
                         }
-                        *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128)) = v0;
-                        *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
-                        *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128)) = u0;
-                        *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane + 32, 128)) = u1;
                     }
                     tc::wg_sync(bar_id, TEAM);
                     my_mu = part[r];
@@ -734,20 +735,30 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     }
                 }
                 float *np = L.num + (long long)L.y * a.ld + L.x;
+                if (Shp::kBoxes == 3 && region) {
+                    // four block steps per round: rows and table entries loaded before the atomics
+                    for (int i0 = half * NI; i0 < half * NI + NI; i0 += 4) {
+                        int2 q[4];
+                        float x0v[4], x1v[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            q[k] = rowtab[b0 + i0 + k];
+                            x0v[k] = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i0 + k, lane, 128));
+                            x1v[k] = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i0 + k, lane + 32, 128));
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (q[k].x >= 0) {
+                                const int o = ((q[k].x >> 16) + ry) * rp + (q[k].x & 0xffff) + cx;
+                                const float ws = __int_as_float(q[k].y) * scale;
+                                atomicAdd(Ri + o, __float2int_rn(x0v[k] * ws));
+                                atomicAdd(Ri + o + 4 * rp, __float2int_rn(x1v[k] * ws));
+                            }
+                    }
+                }
 #pragma unroll 4
                 for (int i = half * NI; i < half * NI + NI; ++i) {
-                    if (Shp::kBoxes == 3 && region) {
-                        const int2 q = rowtab[b0 + i];
-                        if (q.x >= 0) {
-                            const int by = q.x >> 16, bx = q.x & 0xffff;
-                            const float ws = __int_as_float(q.y) * scale;
-                            const float x0v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane, 128));
-                            const float x1v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128));
-                            atomicAdd(Ri + (by + ry) * rp + bx + cx, __float2int_rn(x0v * ws));
-                            atomicAdd(Ri + (by + ry + 4) * rp + bx + cx, __float2int_rn(x1v * ws));
-                        }
-                        continue;
-                    }
+                    if (Shp::kBoxes == 3 && region) break;
                     const bool mi = __shfl_sync(0xffffffffu, mine, i);
                     const float wi = __shfl_sync(0xffffffffu, numW, i);
                     if (region) {

@@ -432,24 +432,27 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         }
                         tc::cp_async_wait_all();
                         tc::wg_sync(bar_id, TEAM);
-#pragma unroll 4
-                        for (int i = half * NI; i < half * NI + NI; ++i) {
-                            const bool mi = __shfl_sync(0xffffffffu, mine, i);
-                            const int by = __shfl_sync(0xffffffffu, L.y, i) - y0, bx = __shfl_sync(0xffffffffu, L.x, i) - x0;
-                            float v0 = 0.f, v1 = 0.f;
-                            if (mi) {
-                                v0 = Rg[(by + ry) * rp + bx + cx];
-                                v1 = Rg[(by + ry + 4) * rp + bx + cx];
+                        // four block steps per round: their loads are issued before any store
+                        for (int i0 = half * NI; i0 < half * NI + NI; i0 += 4) {
+                            float v0[4], v1[4];
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) {
+                                const bool mi = __shfl_sync(0xffffffffu, mine, i0 + k);
+                                const int by = __shfl_sync(0xffffffffu, L.y, i0 + k) - y0;
+                                const int bx = __shfl_sync(0xffffffffu, L.x, i0 + k) - x0;
+                                const int o = mi ? (by + ry) * rp + bx + cx : 0;
+                                v0[k] = mi ? Rg[o] : 0.f;
+                                v1[k] = mi ? Rg[o + 4 * rp] : 0.f;
                             }
-                            {
-                                const float mu = block_mean(v0, v1);
-                                v0 -= mu;
-                                v1 -= mu;
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) {
+                                const int i = i0 + k;
+                                const float mu = block_mean(v0[k], v1[k]);
                                 if (lane == i) my_mu = mu;
                                 if constexpr (SPLIT >= 2) if (lane == 0) part[(pass == 0 ? 128 : 0) + b0 + i] = mu;
+                                *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane, 128)) = v0[k] - mu;
+                                *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1[k] - mu;
                             }
-                            *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane, 128)) = v0;
-                            *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1;
                         }
                         tc::wg_sync(bar_id, TEAM);
                     }
@@ -756,20 +759,34 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                             }
                     }
                 }
+                if (Shp::kBoxes == 1 && region) {
+                    for (int i0 = half * NI; i0 < half * NI + NI; i0 += 4) {
+                        int o[4];
+                        float ws[4], x0v[4], x1v[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const bool mi = __shfl_sync(0xffffffffu, mine, i0 + k);
+                            ws[k] = __shfl_sync(0xffffffffu, numW, i0 + k) * scale;
+                            const int by = __shfl_sync(0xffffffffu, L.y, i0 + k) - y0;
+                            const int bx = __shfl_sync(0xffffffffu, L.x, i0 + k) - x0;
+                            o[k] = mi ? (by + ry) * rp + bx + cx : -1;
+                            x0v[k] = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i0 + k, lane, 128));
+                            x1v[k] = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i0 + k, lane + 32, 128));
+                        }
+#pragma unroll
+                        for (int k = 0; k < 4; ++k)
+                            if (o[k] >= 0) {
+                                atomicAdd(Ri + o[k], __float2int_rn(x0v[k] * ws[k]));
+                                atomicAdd(Ri + o[k] + 4 * rp, __float2int_rn(x1v[k] * ws[k]));
+                            }
+                    }
+                }
 #pragma unroll 4
                 for (int i = half * NI; i < half * NI + NI; ++i) {
-                    if (Shp::kBoxes == 3 && region) break;
+                    if (region) break;
                     const bool mi = __shfl_sync(0xffffffffu, mine, i);
                     const float wi = __shfl_sync(0xffffffffu, numW, i);
-                    if (region) {
-                        const int by = __shfl_sync(0xffffffffu, L.y, i) - y0, bx = __shfl_sync(0xffffffffu, L.x, i) - x0;
-                        if (mi) {
-                            const float x0v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane, 128));
-                            const float x1v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128));
-                            atomicAdd(Ri + (by + ry) * rp + bx + cx, __float2int_rn(x0v * wi * scale));
-                            atomicAdd(Ri + (by + ry + 4) * rp + bx + cx, __float2int_rn(x1v * wi * scale));
-                        }
-                    } else {
+                    {
                         float *ni = reinterpret_cast<float *>(__shfl_sync(0xffffffffu, reinterpret_cast<unsigned long long>(np), i));
                         if (mi) {
                             const float x0v = *reinterpret_cast<const float *>(D + tc::sw128_offset(b0 + i, lane, 128));

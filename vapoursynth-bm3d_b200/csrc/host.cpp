@@ -1034,6 +1034,54 @@ public:
         }
     }
 
+    // ingest of frames fr[0..count) into workspace slots slot0.. in one conversion launch when
+    // their range flags agree (always for float input), else frame by frame
+    void ingest_all(const bm3d_frame *const *fr, int count, bool is_ref, int slot0, const std::vector<bool> &full)
+    {
+        bool same = true;
+        for (int k = 1; k < count; ++k) same = same && full[k] == full[0];
+        const int kind = sample_kind(vi);
+        if (count <= 1 || (!same && kind != SK_F32)) {
+            for (int k = 0; k < count; ++k) ingest(*fr[k], is_ref, slot0 + k, full[k]);
+            return;
+        }
+        const int np = nplanes();
+        const PlaneGeom g{W * bytes_per_sample(vi), H};
+        DevBuf *ws = is_ref ? ws_ref : ws_src;
+        std::vector<PlanePtr> in, out;
+        ConvProgram pr{};
+        if (vi.color_family == BM3D_RGB) {
+            const bool y_only = is_ref && !wiener;
+            for (int k = 0; k < count; ++k) {
+                for (int p = 0; p < 3; ++p) in.push_back(stager_.view(*fr[k], p, g, stream));
+                for (int p = 0; p < (y_only ? 1 : 3); ++p)
+                    out.push_back(PlanePtr{ws[p].as<float>() + (slot0 + k) * fs, (long long)ld * 4});
+            }
+            pr = y_only ? rgb2y_program(kind, vi.bits_per_sample, W, H)
+                        : rgb2opp_program(kind, vi.bits_per_sample, SK_F32, 32, W, H, false);
+        } else {
+            // every plane of the format in one program; planes not needed get no output
+            if (kind == SK_F32) pr = raw_program(SK_F32, np, W, H);
+            else {
+                pr.mode = 0;
+                pr.in_kind = kind;
+                pr.out_kind = SK_F32;
+                pr.nin = pr.nout = np;
+                pr.W = W;
+                pr.H = H;
+                for (int p = 0; p < np; ++p) pr.op[p] = int2float_op(vi.bits_per_sample, full[0], p > 0);
+            }
+            for (int k = 0; k < count; ++k)
+                for (int p = 0; p < np; ++p) {
+                    const bool need = !is_ref ? (process[p] || (p == 0 && !rdef)) : (p == 0 || (wiener && process[p]));
+                    in.push_back(need ? stager_.view(*fr[k], p, g, stream) : PlanePtr{nullptr, 0});
+                    out.push_back(need ? PlanePtr{ws[p].as<float>() + (slot0 + k) * fs, (long long)ld * 4} : PlanePtr{nullptr, 0});
+                }
+        }
+        CU(launch_convert(pr, upload_ptrs(conv_in_[conv_i_], in), upload_ptrs(conv_out_[conv_i_], out), count, stream));
+        conv_i_ = (conv_i_ + 1) % kConvSlots;
+    }
+
     // BM3D_Process_Base::NewFrame / VBM3D_Process_Base::NewFrame property handling
     bool frame_full(const bm3d_frame &fr)
     {
@@ -1349,11 +1397,9 @@ public:
         CU(cudaMemsetAsync(stats, 0, 3 * sizeof(unsigned long long), stream));
         mark(0);
         std::vector<bool> full(count);
-        for (int k = 0; k < count; ++k) {
-            full[k] = frame_full(*src[k]);
-            ingest(*src[k], false, k, full[k]);
-            if (rdef) ingest(*ref[k], true, k, full[k]);
-        }
+        for (int k = 0; k < count; ++k) full[k] = frame_full(*src[k]);
+        ingest_all(src, count, false, 0, full);
+        if (rdef) ingest_all(ref, count, true, 0, full);
         mark(1);
         run_bm(0, count, m_pos.as<uint32_t>(), m_n.as<int>(), m_key.as<float>());
         mark(2);
@@ -1380,9 +1426,34 @@ public:
         fa.B = para.B;
         CU(launch_finalize(fa, count, stream));
         mark(5);
-        // egress
+        // egress: one conversion launch for the batch when every plane is processed and the
+        // frames' range flags agree (or the output is float), else frame by frame
         const int kind = sample_kind(vi);
+        bool batch = count > 1;
+        for (int k = 1; k < count; ++k) batch = batch && (full[k] == full[0] || kind == SK_F32);
+        for (int p = 0; p < np; ++p) batch = batch && (process[p] || vi.color_family == BM3D_RGB);
+        if (batch) {
+            std::vector<PlanePtr> i1, o1;
+            ConvProgram pr{};
+            for (int k = 0; k < count; ++k)
+                for (int p = 0; p < np; ++p) {
+                    i1.push_back(PlanePtr{acc_num[p].as<float>() + k * fs, (long long)ld * 4});
+                    o1.push_back(stager_.target(*dst[k], p, g));
+                }
+            if (vi.color_family == BM3D_RGB) pr = opp2rgb_program(SK_F32, 32, kind, vi.bits_per_sample, W, H);
+            else if (kind == SK_F32) pr = raw_program(SK_F32, np, W, H);
+            else {
+                pr.mode = 0; pr.in_kind = SK_F32; pr.out_kind = kind; pr.nin = pr.nout = np; pr.W = W; pr.H = H;
+                for (int p = 0; p < np; ++p) pr.op[p] = float2int_op(vi.bits_per_sample, full[0], p > 0);
+            }
+            CU(launch_convert(pr, upload_ptrs(conv_in_[conv_i_], i1), upload_ptrs(conv_out_[conv_i_], o1), count, stream));
+            conv_i_ = (conv_i_ + 1) % kConvSlots;
+        }
         for (int k = 0; k < count; ++k) {
+            if (batch) {
+                copy_props(src[k], dst[k]);
+                continue;
+            }
             std::vector<PlanePtr> i1, o1;
             if (vi.color_family == BM3D_RGB) {
                 for (int p = 0; p < 3; ++p) i1.push_back(PlanePtr{acc_num[p].as<float>() + k * fs, (long long)ld * 4});
@@ -1512,13 +1583,12 @@ public:
         for (int i = 0; i < nwin; ++i) full[i] = true;
         for (int k = 0; k < count; ++k) full[n + k - first] = frame_full(*src[n + k - first]);
         mark(0);
-        for (int i = 0; i < nwin; ++i) {
-            // Int2Float of window frames uses the current frame's range flag; frames outside the
-            // output batch use their own (identical for constant-range clips)
-            const bool fl = (i >= n - first && i < n - first + count) ? full[i] : frame_full_quiet(*src[i]);
-            ingest(*src[i], false, i, fl);
-            if (rdef) ingest(*ref[i], true, i, fl);
-        }
+        // Int2Float of window frames uses the current frame's range flag; frames outside the
+        // output batch use their own (identical for constant-range clips)
+        for (int i = 0; i < nwin; ++i)
+            if (!(i >= n - first && i < n - first + count)) full[i] = frame_full_quiet(*src[i]);
+        ingest_all(src, nwin, false, 0, full);
+        if (rdef) ingest_all(ref, nwin, true, 0, full);
         mark(1);
         // learned form: descriptors of every window frame, for the current-frame proposals and
         // for the other frames' predictive search

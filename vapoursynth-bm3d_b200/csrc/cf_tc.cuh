@@ -108,6 +108,38 @@ __device__ __forceinline__ float block_mean(float v0, float v1)
     return s * (1.0f / 64.0f);
 }
 
+// means of N blocks (N = 4 or 8) whose pixels a warp holds two per lane, s[k] = the lane's sum for
+// block k: log2(N) halving steps (each lane keeps half of its values and receives the other half
+// of its partner's) leave one block's partial sum per lane, the remaining steps finish it, and
+// one shuffle per block brings every mean to every lane (9 + 8 shuffles for 8 blocks instead of 40)
+template <int N>
+__device__ __forceinline__ void block_means(float (&s)[N], int lane)
+{
+    constexpr int L = N == 8 ? 3 : 2;
+#pragma unroll
+    for (int st = 0; st < L; ++st) {
+        const int off = 16 >> st, h = N >> (st + 1);
+        const bool up = (lane & off) != 0;
+#pragma unroll
+        for (int k = 0; k < h; ++k) {
+            const float keep = up ? s[k + h] : s[k];
+            const float send = up ? s[k] : s[k + h];
+            s[k] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+        }
+    }
+    float w = s[0];
+#pragma unroll
+    for (int off = 16 >> L; off > 0; off >>= 1) w += __shfl_xor_sync(0xffffffffu, w, off);
+    // block v's sum is held by the lanes whose bits (4, 3[, 2]) spell v's bits from the top
+#pragma unroll
+    for (int v = 0; v < N; ++v) {
+        int src = 0;
+#pragma unroll
+        for (int st = 0; st < L; ++st) src |= ((v >> (L - 1 - st)) & 1) << (4 - st);
+        s[v] = __shfl_sync(0xffffffffu, w, src) * (1.0f / 64.0f);
+    }
+}
+
 template <int G, bool WIENER>
 __global__ void __launch_bounds__(TcShape<G, WIENER>::kTeam * TcShape<G, WIENER>::kWG, 1)
 cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
@@ -353,6 +385,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     // fp64 tables after the tensor-core image: C8[u][y] = 2 cos(pi (2y + 1) u / 16), then the
     // z matrix Dz[kz][b] = 2 cos(pi (2b + 1) kz / 2G) (hard-threshold recheck and block means)
     const double *xtab = reinterpret_cast<const double *>(reinterpret_cast<const unsigned char *>(tables) + Lay::kTableBytes);
+    // then, in fp32, Dz as [b][kz] (dzt) and the inverse z matrix Ci[b][kz] as [kz][b] (dzi;
+    // Ci[b][0] = 1, Ci[b][kz] = Dz[kz][b]): a warp's lanes read consecutive words
+    const float *dzt = reinterpret_cast<const float *>(xtab + 64 + G * G);
+    const float *dzi = dzt + G * G;
     unsigned long long n_recheck = 0, n_changed = 0;
 
     bool failed = false;
@@ -400,14 +436,21 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                             u0[k] = mi ? Br[o] : 0.f;
                             u1[k] = mi ? Br[o + 4 * rp] : 0.f;
                         }
+                        float m8[8];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            m8[k] = v0[k] + v1[k];
+                            m8[4 + k] = u0[k] + u1[k];
+                        }
+                        block_means<8>(m8, lane);
+                        if (lane == 0) {
+                            *reinterpret_cast<float4 *>(part + b0 + i0) = make_float4(m8[0], m8[1], m8[2], m8[3]);
+                            *reinterpret_cast<float4 *>(part + 128 + b0 + i0) = make_float4(m8[4], m8[5], m8[6], m8[7]);
+                        }
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
                             const int i = i0 + k;
-                            const float ms = block_mean(v0[k], v1[k]), mr = block_mean(u0[k], u1[k]);
-                            if (lane == 0) {
-                                part[b0 + i] = ms;
-                                part[128 + b0 + i] = mr;
-                            }
+                            const float ms = m8[k], mr = m8[4 + k];
                             *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128)) = v0[k] - ms;
                             *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1[k] - ms;
                             *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128)) = u0[k] - mr;
@@ -444,12 +487,18 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                                 v0[k] = mi ? Rg[o] : 0.f;
                                 v1[k] = mi ? Rg[o + 4 * rp] : 0.f;
                             }
+                            float m4[4];
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) m4[k] = v0[k] + v1[k];
+                            block_means<4>(m4, lane);
+                            if constexpr (SPLIT >= 2)
+                                if (lane == 0)
+                                    *reinterpret_cast<float4 *>(part + (pass == 0 ? 128 : 0) + b0 + i0) = make_float4(m4[0], m4[1], m4[2], m4[3]);
 #pragma unroll
                             for (int k = 0; k < 4; ++k) {
                                 const int i = i0 + k;
-                                const float mu = block_mean(v0[k], v1[k]);
+                                const float mu = m4[k];
                                 if (lane == i) my_mu = mu;
-                                if constexpr (SPLIT >= 2) if (lane == 0) part[(pass == 0 ? 128 : 0) + b0 + i] = mu;
                                 *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane, 128)) = v0[k] - mu;
                                 *reinterpret_cast<float *>(dst + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1[k] - mu;
                             }
@@ -538,19 +587,32 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
 #pragma unroll
             for (int k = 0; k < 3; ++k) thr[k] = WIENER ? 0.0f : a.thr4[p][G - 1][(j == 0) + k];
             // (hard threshold) the exact z transform of the block means' (0, 0) coefficients 256 mu
+            // (only the first column half holds column 0)
             float dcz = 0.0f, dczr = 0.0f;
             uint64_t flags = 0;                        // columns (relative to cb) to recompute
-            {
+            if constexpr (SPLIT >= 2) {
+                if (half == 0) {
+                    // the group's means from shared memory, four per broadcast load
+                    const float4 *m4 = reinterpret_cast<const float4 *>(part + (r / G) * G);
+#pragma unroll 2
+                    for (int b4 = 0; b4 < G / 4; ++b4) {
+                        const float4 m = m4[b4];
+                        float4 mr = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if constexpr (WIENER) mr = m4[32 + b4];
+                        const float d0 = __ldg(dzt + (4 * b4) * G + j), d1 = __ldg(dzt + (4 * b4 + 1) * G + j);
+                        const float d2 = __ldg(dzt + (4 * b4 + 2) * G + j), d3 = __ldg(dzt + (4 * b4 + 3) * G + j);
+                        dcz = fmaf(d0, m.x, fmaf(d1, m.y, fmaf(d2, m.z, fmaf(d3, m.w, dcz))));
+                        if constexpr (WIENER) dczr = fmaf(d0, mr.x, fmaf(d1, mr.y, fmaf(d2, mr.z, fmaf(d3, mr.w, dczr))));
+                    }
+                }
+            } else {
                 const int gl = (lane / G) * G;         // lane of the group's first block
 #pragma unroll 4
-                for (int b = 0; b < G; ++b) {
-                    const float dzb = (float)__ldg(xtab + 64 + j * G + b);
-                    dcz = fmaf(dzb, __shfl_sync(0xffffffffu, my_mu, gl + b), dcz);
-                    if constexpr (WIENER) dczr = fmaf(dzb, __shfl_sync(0xffffffffu, my_mur, gl + b), dczr);
-                }
-                dcz *= 256.0f;
-                dczr *= 256.0f;
+                for (int b = 0; b < G; ++b)
+                    dcz = fmaf(__ldg(dzt + b * G + j), __shfl_sync(0xffffffffu, my_mu, gl + b), dcz);
             }
+            dcz *= 256.0f;
+            dczr *= 256.0f;
             // the recheck interval [lo, hi] of |c| around each of the three threshold classes
             float tlo[3], thi[3];
 #pragma unroll
@@ -693,13 +755,21 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 // the inverse of the (0, 0) coefficients: block j of the group gets
                 // sum_kz Ci[j][kz] S(kz, 0, 0), Ci[j][0] = 1, Ci[j][kz] = Dz[kz][j]
                 float dcb = 0.0f;
-                {
+                if constexpr (SPLIT >= 2) {
+                    const float4 *s4 = reinterpret_cast<const float4 *>(part + (r / G) * G);
+#pragma unroll 2
+                    for (int k4 = 0; k4 < G / 4; ++k4) {
+                        const float4 sk = s4[k4];
+                        dcb = fmaf(__ldg(dzi + (4 * k4) * G + j), sk.x, dcb);
+                        dcb = fmaf(__ldg(dzi + (4 * k4 + 1) * G + j), sk.y, dcb);
+                        dcb = fmaf(__ldg(dzi + (4 * k4 + 2) * G + j), sk.z, dcb);
+                        dcb = fmaf(__ldg(dzi + (4 * k4 + 3) * G + j), sk.w, dcb);
+                    }
+                } else {
                     const int gl = (lane / G) * G;
 #pragma unroll 4
-                    for (int kz = 0; kz < G; ++kz) {
-                        const float sk = SPLIT == 1 ? __shfl_sync(0xffffffffu, s00, gl + kz) : part[(r / G) * G + kz];
-                        dcb = fmaf(kz == 0 ? 1.0f : (float)__ldg(xtab + 64 + kz * G + j), sk, dcb);
-                    }
+                    for (int kz = 0; kz < G; ++kz)
+                        dcb = fmaf(__ldg(dzi + kz * G + j), __shfl_sync(0xffffffffu, s00, gl + kz), dcb);
                 }
                 tc::tmem_wait_ld();
 #pragma unroll

@@ -966,6 +966,18 @@ public:
             const size_t base = img.size();
             img.resize(base + xt.size() * sizeof(double));
             std::memcpy(img.data() + base, xt.data(), xt.size() * sizeof(double));
+            // then, in fp32 for the per-block DC terms, the forward z matrix as [b][kz] and the
+            // inverse one (Dz with row 0 replaced by ones) as [kz][b]: the lanes of a warp
+            // (consecutive kz, resp. b) read consecutive words
+            std::vector<float> ft;
+            const double *dz = xt.data() + 64;
+            for (int b = 0; b < para.G; ++b)
+                for (int kz = 0; kz < para.G; ++kz) ft.push_back((float)dz[kz * para.G + b]);
+            for (int kz = 0; kz < para.G; ++kz)
+                for (int b = 0; b < para.G; ++b) ft.push_back(kz == 0 ? 1.0f : (float)dz[kz * para.G + b]);
+            const size_t fbase = img.size();
+            img.resize(fbase + ft.size() * sizeof(float));
+            std::memcpy(img.data() + fbase, ft.data(), ft.size() * sizeof(float));
             CU(cudaMemcpy(tc_tab.get(img.size()), img.data(), img.size(), cudaMemcpyHostToDevice));
             CU(cudaMemset(tc_status.get(sizeof(int)), 0, sizeof(int)));
         }

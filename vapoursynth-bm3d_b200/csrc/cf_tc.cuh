@@ -226,11 +226,15 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     uint64_t *mb = &mbar[wg];
     uint32_t phase = 0;
 
+    // Only the issuing warp polls the mbarrier; the team's other warps sleep in the barrier that
+    // passes its verdict on, instead of taking issue slots from the other team with their polls.
     auto wait_mma = [&]() -> bool {
-        const bool ok = tc::mbar_wait_bounded(mb, phase, kTcWaitLimit);
+        bool ok = true;
+        if (t < 32) ok = tc::mbar_wait_bounded(mb, phase, kTcWaitLimit);
         phase ^= 1u;
+        const bool all = tc::wg_and(bar_id, TEAM, ok);
         tc::fence_after_sync();
-        return tc::wg_and(bar_id, TEAM, ok);
+        return all;
     };
     auto publish = [&]() {
         tc::fence_proxy_async_smem();

@@ -413,18 +413,40 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             if (!a.process[p]) continue;
             const GroupLoc L = locate(a, p, g0, pk);
             const bool last = next_plane(p + 1) >= 3;
-            // Every block enters the products with its mean removed (source and, for the Wiener
-            // filter, reference), so that the tf32 rounding scales with the block's detail, not
-            // its level; the means' own transform (the (0, 0) coefficients of every z frequency)
-            // is added back in fp32 before the shrinkage.  Likewise the shrunk (0, 0) coefficients
-            // leave the inverse products and come back as one fp32 constant per block.
+            // Every block enters the products with a level removed, so that the tf32 rounding
+            // scales with the block's detail, not its level.  Hard threshold: each block's own
+            // mean; the means' transform (the (0, 0) coefficients of every z frequency) is added
+            // back in fp32 before the shrinkage and the shrunk (0, 0) coefficients leave the
+            // inverse products and come back as one fp32 constant per block.  Wiener filter: one
+            // level per group (the mean of its first block, source and reference), which only
+            // the (0, 0, 0) coefficient carries: 512 G times the level, added back exactly, and
+            // the shrunk (0, 0, 0) coefficient alone leaves the inverse products.
             float my_mu = 0.0f, my_mur = 0.0f;
+            // (Wiener) groups of this warp's block steps and the first row of the first one
+            constexpr int GW = NI / G > 1 ? NI / G : 1;
+            const int gfirst = ((b0 + half * NI) / G) * G;
             // 1. gather (rows of foreign or partial groups are zero), one block per warp step
             if (region) {
                 if constexpr (Shp::kBoxes == 3) {
                     if (half == 0) rowtab[r].x = mine ? ((L.y - y0) << 16) | (L.x - x0) : -1;
                     tc::cp_async_wait_all();
                     tc::wg_sync(bar_id, TEAM);
+                    // (the three-box form is the Wiener filter's) the levels of this warp's groups
+                    float lv[4];
+#pragma unroll
+                    for (int k = 0; k < 2; ++k) {
+                        const int pq = k < GW ? rowtab[gfirst + k * G].x : -1;
+                        const int o = pq >= 0 ? ((pq >> 16) + ry) * rp + (pq & 0xffff) + cx : 0;
+                        lv[2 * k] = pq >= 0 ? Bs[o] + Bs[o + 4 * rp] : 0.f;
+                        lv[2 * k + 1] = pq >= 0 ? Br[o] + Br[o + 4 * rp] : 0.f;
+                    }
+                    block_means<4>(lv, lane);
+                    if (lane == 0)
+#pragma unroll
+                        for (int k = 0; k < GW; ++k) {
+                            part[gfirst + k * G] = lv[2 * k];
+                            part[128 + gfirst + k * G] = lv[2 * k + 1];
+                        }
                     // four block steps per round: their loads are issued before any store
                     for (int i0 = half * NI; i0 < half * NI + NI; i0 += 4) {
                         int pq[4];
@@ -440,21 +462,11 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                             u0[k] = mi ? Br[o] : 0.f;
                             u1[k] = mi ? Br[o + 4 * rp] : 0.f;
                         }
-                        float m8[8];
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            m8[k] = v0[k] + v1[k];
-                            m8[4 + k] = u0[k] + u1[k];
-                        }
-                        block_means<8>(m8, lane);
-                        if (lane == 0) {
-                            *reinterpret_cast<float4 *>(part + b0 + i0) = make_float4(m8[0], m8[1], m8[2], m8[3]);
-                            *reinterpret_cast<float4 *>(part + 128 + b0 + i0) = make_float4(m8[4], m8[5], m8[6], m8[7]);
-                        }
 #pragma unroll
                         for (int k = 0; k < 4; ++k) {
                             const int i = i0 + k;
-                            const float ms = m8[k], mr = m8[4 + k];
+                            const bool g1 = GW > 1 && b0 + i - gfirst >= G;
+                            const float ms = g1 ? lv[2] : lv[0], mr = g1 ? lv[3] : lv[1];
                             *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128)) = v0[k] - ms;
                             *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1[k] - ms;
                             *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128)) = u0[k] - mr;
@@ -462,8 +474,6 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         }
                     }
                     tc::wg_sync(bar_id, TEAM);
-                    my_mu = part[r];
-                    my_mur = part[128 + r];
                     // the next plane's boxes load while this plane is filtered
                     if (!last) load_boxes(cur, next_plane(p + 1));
                 } else {
@@ -479,6 +489,23 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         }
                         tc::cp_async_wait_all();
                         tc::wg_sync(bar_id, TEAM);
+                        // (Wiener) the levels of this warp's groups in this plane
+                        float lp[4] = {0.f, 0.f, 0.f, 0.f};
+                        if constexpr (WIENER) {
+#pragma unroll
+                            for (int k = 0; k < 2; ++k) {
+                                const int sl = (gfirst + k * G - b0) & 31;
+                                const bool mi = __shfl_sync(0xffffffffu, mine, sl) && k < GW;
+                                const int by = __shfl_sync(0xffffffffu, L.y, sl) - y0;
+                                const int bx = __shfl_sync(0xffffffffu, L.x, sl) - x0;
+                                const int o = mi ? (by + ry) * rp + bx + cx : 0;
+                                lp[k] = mi ? Rg[o] + Rg[o + 4 * rp] : 0.f;
+                            }
+                            block_means<4>(lp, lane);
+                            if (lane == 0)
+#pragma unroll
+                                for (int k = 0; k < GW; ++k) part[(pass == 0 ? 128 : 0) + gfirst + k * G] = lp[k];
+                        }
                         // four block steps per round: their loads are issued before any store
                         for (int i0 = half * NI; i0 < half * NI + NI; i0 += 4) {
                             float v0[4], v1[4];
@@ -492,12 +519,17 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                                 v1[k] = mi ? Rg[o + 4 * rp] : 0.f;
                             }
                             float m4[4];
+                            if constexpr (WIENER) {
 #pragma unroll
-                            for (int k = 0; k < 4; ++k) m4[k] = v0[k] + v1[k];
-                            block_means<4>(m4, lane);
-                            if constexpr (SPLIT >= 2)
-                                if (lane == 0)
-                                    *reinterpret_cast<float4 *>(part + (pass == 0 ? 128 : 0) + b0 + i0) = make_float4(m4[0], m4[1], m4[2], m4[3]);
+                                for (int k = 0; k < 4; ++k) m4[k] = GW > 1 && b0 + i0 + k - gfirst >= G ? lp[1] : lp[0];
+                            } else {
+#pragma unroll
+                                for (int k = 0; k < 4; ++k) m4[k] = v0[k] + v1[k];
+                                block_means<4>(m4, lane);
+                                if constexpr (SPLIT >= 2)
+                                    if (lane == 0)
+                                        *reinterpret_cast<float4 *>(part + b0 + i0) = make_float4(m4[0], m4[1], m4[2], m4[3]);
+                            }
 #pragma unroll
                             for (int k = 0; k < 4; ++k) {
                                 const int i = i0 + k;
@@ -509,10 +541,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         }
                         tc::wg_sync(bar_id, TEAM);
                     }
-                    if constexpr (SPLIT >= 2) {
-                        my_mu = part[r];
-                        if constexpr (WIENER) my_mur = part[128 + r];
-                    }
+                    if constexpr (SPLIT >= 2) my_mu = part[r];
                 }
             } else {
                 const float *sp = L.src + (long long)L.y * a.ld + L.x;
@@ -542,6 +571,30 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     }
                 }
                 tc::cp_async_wait_all();
+                float lp[4] = {0.f, 0.f, 0.f, 0.f};
+                if constexpr (WIENER) {
+                    // the levels of this warp's groups (a group's first block may have been copied
+                    // by the other warp of the quarter)
+                    tc::wg_sync(bar_id, TEAM);
+#pragma unroll
+                    for (int k = 0; k < 2; ++k)
+#pragma unroll
+                        for (int op = 0; op < 2; ++op) {
+                            const int row = k < GW ? gfirst + k * G : gfirst;
+                            const float *d0 = reinterpret_cast<const float *>(D + op * Lay::kXBytes + tc::sw128_offset(row, lane, 128));
+                            const float *d1 = reinterpret_cast<const float *>(D + op * Lay::kXBytes + tc::sw128_offset(row, lane + 32, 128));
+                            lp[2 * k + op] = k < GW ? *d0 + *d1 : 0.f;
+                        }
+                    block_means<4>(lp, lane);
+                    if (lane == 0)
+#pragma unroll
+                        for (int k = 0; k < GW; ++k) {
+                            part[gfirst + k * G] = lp[2 * k];
+                            part[128 + gfirst + k * G] = lp[2 * k + 1];
+                        }
+                    // every warp has read its levels before any block is changed
+                    tc::wg_sync(bar_id, TEAM);
+                }
                 // each lane re-reads only the elements its own copies wrote
 #pragma unroll 4
                 for (int i = half * NI; i < half * NI + NI; ++i) {
@@ -549,18 +602,28 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     for (int op = 0; op < (WIENER ? 2 : 1); ++op) {
                         float *d0 = reinterpret_cast<float *>(D + op * Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128));
                         float *d1 = reinterpret_cast<float *>(D + op * Lay::kXBytes + tc::sw128_offset(b0 + i, lane + 32, 128));
-                        const float mu = block_mean(*d0, *d1);
+                        float mu;
+                        if constexpr (WIENER) {
+                            const bool g1 = GW > 1 && b0 + i - gfirst >= G;
+                            mu = g1 ? lp[2 + op] : lp[op];
+                        } else {
+                            mu = block_mean(*d0, *d1);
+                            if constexpr (SPLIT >= 2) if (lane == 0) part[b0 + i] = mu;
+                        }
                         *d0 -= mu;
                         *d1 -= mu;
                         if (op == 0 && lane == i) my_mu = mu;
-                        if constexpr (SPLIT >= 2) if (lane == 0) part[128 * op + b0 + i] = mu;
                     }
                 }
                 if constexpr (SPLIT >= 2) {
                     tc::wg_sync(bar_id, TEAM);
                     my_mu = part[r];
-                    if constexpr (WIENER) my_mur = part[128 + r];
                 }
+            }
+            // (Wiener) the group's levels, read before the shrinkage reuses the scratch row
+            if constexpr (WIENER) {
+                my_mu = part[r];
+                my_mur = part[128 + r];
             }
             if (last) {
                 bound_tile(nxt);
@@ -594,19 +657,22 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             // (only the first column half holds column 0)
             float dcz = 0.0f, dczr = 0.0f;
             uint64_t flags = 0;                        // columns (relative to cb) to recompute
-            if constexpr (SPLIT >= 2) {
+            if constexpr (WIENER) {
+                // the group's levels: sum_b Dz[0][b] = 2 G, sum_b Dz[kz][b] = 0 for kz > 0
+                if (half == 0 && j == 0) {
+                    dcz = my_mu * (float)(2 * G);
+                    dczr = my_mur * (float)(2 * G);
+                }
+            } else if constexpr (SPLIT >= 2) {
                 if (half == 0) {
                     // the group's means from shared memory, four per broadcast load
                     const float4 *m4 = reinterpret_cast<const float4 *>(part + (r / G) * G);
 #pragma unroll 2
                     for (int b4 = 0; b4 < G / 4; ++b4) {
                         const float4 m = m4[b4];
-                        float4 mr = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if constexpr (WIENER) mr = m4[32 + b4];
                         const float d0 = __ldg(dzt + (4 * b4) * G + j), d1 = __ldg(dzt + (4 * b4 + 1) * G + j);
                         const float d2 = __ldg(dzt + (4 * b4 + 2) * G + j), d3 = __ldg(dzt + (4 * b4 + 3) * G + j);
                         dcz = fmaf(d0, m.x, fmaf(d1, m.y, fmaf(d2, m.z, fmaf(d3, m.w, dcz))));
-                        if constexpr (WIENER) dczr = fmaf(d0, mr.x, fmaf(d1, mr.y, fmaf(d2, mr.z, fmaf(d3, mr.w, dczr))));
                     }
                 }
             } else {
@@ -712,9 +778,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     }
                 }
             }
-            // the shrunk (0, 0) coefficient of this row leaves the inverse products
+            // the shrunk (0, 0) coefficient of this row (Wiener: of the group's kz = 0 row) leaves
+            // the inverse products
             float s00 = 0.0f;
-            if (cb == 0) {
+            if (cb == 0 && (!WIENER || j == 0)) {
                 float *s0p = reinterpret_cast<float *>(D + tc::sw128_offset(0, r, 64));
                 s00 = *s0p;
                 *s0p = 0.0f;
@@ -759,7 +826,9 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 // the inverse of the (0, 0) coefficients: block j of the group gets
                 // sum_kz Ci[j][kz] S(kz, 0, 0), Ci[j][0] = 1, Ci[j][kz] = Dz[kz][j]
                 float dcb = 0.0f;
-                if constexpr (SPLIT >= 2) {
+                if constexpr (WIENER) {
+                    dcb = part[(r / G) * G];           // the inverse of S(0, 0, 0) alone: a constant
+                } else if constexpr (SPLIT >= 2) {
                     const float4 *s4 = reinterpret_cast<const float4 *>(part + (r / G) * G);
 #pragma unroll 2
                     for (int k4 = 0; k4 < G / 4; ++k4) {

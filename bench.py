@@ -85,6 +85,15 @@ def cpu_sample(threads, frames, width, rows):
     return mpix, dt, f"{frames} frame crops of {width}x{rows} (rows 0..{rows - 1} of the config frames), one per thread"
 
 
+def workload_config(frames, width, height, world):
+    """The workload as both arms report it (the form that produced the number is a separate key)."""
+    mb = frames * width * height * 3 * 4 / 1e6
+    l2 = (f"inputs larger than L2 ({mb:.0f} MB of input frames, ~{10 * mb / 1e3:.0f} GB working set per step)"
+          if mb > 126 else f"inputs smaller than L2 ({mb:.0f} MB of input frames): a short run, not the headline size")
+    return {"workload": WORKLOAD, "frames_per_gpu": frames, "width": width, "height": height,
+            "parallelism": f"frame-sharded replicas x{world}", "l2": l2}
+
+
 def reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -102,7 +111,7 @@ def reference_arm(args):
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mpix/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 2), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "frames_per_gpu": args.frames, "width": args.width, "height": args.height},
+        "config": workload_config(args.frames, args.width, args.height, world),
         "cpu_baseline": {"value": round(value, 4), "unit": "Mpix/s", "cores": threads, "kind": "port",
                          "sample": sample + "; CPU oracle (bm3d_oracle.cpp) restating the reference's path, "
                                             "FFTW replaced by a separable FP32 DCT"},
@@ -494,9 +503,7 @@ def ours_arm(args):
             "warmup": args.warmup, "ms_per_step": round(R["ms"], 3), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if head == "fp32" else "f32 (tf32 tensor-core transforms)",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "form": head, "frames_per_gpu": F, "width": Wd, "height": Hd,
-                       "parallelism": f"frame-sharded replicas x{world}",
-                       "l2": "inputs larger than L2 (199 MB of input frames, ~2 GB working set per step)"},
+            "config": workload_config(F, Wd, Hd, world), "form": head,
             "forms": {"fp32": form_summary("fp32"), "tf32": form_summary("tf32"),
                       "tf32_final": form_summary("tf32_final"), "learned": form_summary("learned"),
                       "psnr_delta_db": round(dpsnr, 4), "speedup": round(res["fp32"]["ms"] / res["tf32"]["ms"], 3),

@@ -13,7 +13,9 @@ the plain transform, the Final one runs on the tensor cores) and the learned-pro
 network).  `value` is the fastest of the tensor-core forms whose output PSNR against the clean
 frames stays within 0.05 dB of the plain path's (else the plain path's); `forms` gives all four.  `value` times the device-resident pipeline (frames
 already in HBM); `e2e` times the same calls with pinned host frames (host->device and
-device->host copies inside the timed region).
+device->host copies inside the timed region), made as a frame server makes them: two host threads,
+each with its own filter instances and stream, request half of the frames each, so that one
+half's copies overlap the other half's kernels.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -275,10 +277,11 @@ class Pipeline:
             L.bm3d_set_stream(st.h, C.c_void_p(stream.cuda_stream))
         self.L, self.capi = L, capi
 
-    def run(self, F, a_in, a_opp, a_basic, a_final, a_out):
+    def run(self, F, a_in, a_opp, a_basic, a_final, a_out, n=0):
+        """Output frames [n, n + F); the arrays hold those F frames."""
         for (st, src, ref, dst) in ((self.opp, a_in, None, a_opp), (self.basic, a_opp, None, a_basic),
                                     (self.final, a_opp, a_basic, a_final), (self.rgb, a_final, None, a_out)):
-            if self.L.bm3d_get_frames_async(st.h, 0, F, src, ref, dst) != 0:
+            if self.L.bm3d_get_frames_async(st.h, n, F, src, ref, dst) != 0:
                 raise RuntimeError(self.capi.last_error())
 
 
@@ -308,9 +311,8 @@ def ours_arm(args):
     # forms: the plain drop-in; tensor cores in both filters; the hard-threshold filter in FP32
     # (exact decisions, and faster than its tensor-core version) with the tensor-core Final; and
     # the learned proposals
-    pipes = {"fp32": Pipeline(L, capi, vi, stream, "fp32"), "tf32": Pipeline(L, capi, vi, stream, "tf32"),
-             "tf32_final": Pipeline(L, capi, vi, stream, ("fp32", "tf32")),
-             "learned": Pipeline(L, capi, vi, stream, "learned")}
+    precisions = {"fp32": "fp32", "tf32": "tf32", "tf32_final": ("fp32", "tf32"), "learned": "learned"}
+    pipes = {form: Pipeline(L, capi, vi, stream, pr) for form, pr in precisions.items()}
 
     def planes(n):
         return [[torch.empty((Hd, Wd), dtype=torch.float32, device="cuda") for _ in range(3)] for _ in range(n)]
@@ -327,17 +329,26 @@ def ours_arm(args):
     h_in = torch.from_numpy(nz).pin_memory()
     h_out = torch.empty_like(h_in).pin_memory()
     H_ = capi.MEM_HOST
-    _, ah_in = make_frames(capi, [[h_in[k, p] for p in range(3)] for k in range(F)], H_)
-    _, ah_out = make_frames(capi, [[h_out[k, p] for p in range(3)] for k in range(F)], H_)
+    # end to end as a frame server runs it: two host threads, each with its own filter instances on
+    # its own stream, request half of the frames each, so that one half's copies overlap the other
+    # half's kernels (the calls with host frames block until their results are on the host)
+    hf = (F + 1) // 2
+    halves = []
+    for lo, hi in (((0, hf), (hf, F)) if F > 1 else ((0, F),)):
+        arrs = tuple(make_frames(capi, fr[lo:hi], kind)[1] for fr, kind in (
+            ([[h_in[k, p] for p in range(3)] for k in range(F)], H_), (f_opp, D), (f_basic, D), (f_final, D),
+            ([[h_out[k, p] for p in range(3)] for k in range(F)], H_)))
+        halves.append((lo, hi - lo, arrs))
+    stream2 = torch.cuda.Stream()
+    pipes2 = {}
 
     def barrier():
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
 
-    def timed(pipe, host, steps, warmup, profile=False):
-        fn = (lambda: pipe.run(F, ah_in, a_opp, a_basic, a_final, ah_out)) if host else \
-             (lambda: pipe.run(F, a_in, a_opp, a_basic, a_final, a_out))
+    def timed(pipe, steps, warmup, profile=False):
+        fn = lambda: pipe.run(F, a_in, a_opp, a_basic, a_final, a_out)  # noqa: E731
         for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
@@ -375,6 +386,53 @@ def ours_arm(args):
             ms = float(t.item())
         return ms, {k: [v / steps for v in vs] for k, vs in stage.items()}, launches // steps
 
+    def timed_e2e(form, steps, warmup):
+        """Host frames in and out, half of the frames per host thread (`halves`); CUDA events on the
+        first stream bracket both streams' work."""
+        if form not in pipes2:
+            pipes2[form] = Pipeline(L, capi, vi, stream2, precisions[form])
+        workers = [pipes[form], pipes2[form]]
+        errors = []
+
+        def half(i):
+            n, cnt, arrs = halves[i]
+            try:
+                workers[i].run(cnt, *arrs, n=n)
+            except Exception as e:  # noqa: BLE001 -- reported on the main thread
+                errors.append(e)
+
+        def step():
+            ts = [threading.Thread(target=half, args=(i,)) for i in range(len(halves))]
+            for t in ts:
+                t.start()
+            for t in ts:
+                t.join()
+            if errors:
+                raise errors[0]
+
+        for _ in range(warmup):
+            step()
+        barrier()
+        e0, e1, eb = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+                      torch.cuda.Event())
+        total = 0.0
+        for _ in range(steps):
+            e0.record(stream)
+            stream2.wait_event(e0)
+            step()
+            eb.record(stream2)
+            stream.wait_event(eb)
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+        barrier()
+        ms = total / steps
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
     def psnr_of(out):
         return 10 * np.log10(1.0 / float(np.mean((out.astype(np.float64) - clean) ** 2)))
 
@@ -383,10 +441,14 @@ def ours_arm(args):
     clocks = Clocks(local)
     clocks.start()
     for form, pipe in pipes.items():
-        ms, stage, launches = timed(pipe, False, args.steps, args.warmup, profile=True)
+        ms, stage, launches = timed(pipe, args.steps, args.warmup, profile=True)
         out = torch.stack([torch.stack(f) for f in f_out]).cpu().numpy()
-        ms_plain, _, _ = timed(pipe, False, args.steps, 1, profile=False)
-        ms_e2e, _, _ = timed(pipe, True, args.steps, args.warmup, profile=False)
+        ms_plain, _, _ = timed(pipe, args.steps, 1, profile=False)
+        ms_e2e = timed_e2e(form, args.steps, args.warmup)
+        # one more whole-batch run, so that the instances' counters and lists read below describe
+        # the 8-frame step (the end-to-end calls left half a batch in them)
+        pipe.run(F, a_in, a_opp, a_basic, a_final, a_out)
+        torch.cuda.synchronize()
         res[form] = dict(ms=ms, stage=stage, launches=launches, psnr=psnr_of(out), ms_unprofiled=ms_plain, ms_e2e=ms_e2e)
     clk = clocks.stop()
     psnr_in = psnr_of(nz)

@@ -163,18 +163,44 @@ __device__ __noinline__ void wiener_column(float *Wc, float sg)
 }
 
 // Non-power-of-two group length n (< G): direct FMA chains over the n x n tables (the oracle's
-// fdct_direct / idct_direct).
+// fdct_direct / idct_direct), t[k][0] x[0] then fused multiply-adds over j = 1 .. n - 1 for every
+// output k.  Eight outputs advance together, so that each step reads x[j] once (from shared
+// memory) and runs eight independent chains; the arrays indexed by k (the spectrum, the outputs
+// of the inverse) are touched O(n) times only.
+constexpr int kDirectChains = 8;
+
+// out[k] = sum_j t[k][j] x[j] for k < n, x[j] = in[j * kTP]; first term a product, as above
+__device__ __forceinline__ void direct_sums(const float *in, const float *t, int n, bool first_mul, float *out)
+{
+    for (int k0 = 0; k0 < n; k0 += kDirectChains) {
+        float acc[kDirectChains];
+        const float x0 = in[0];
+#pragma unroll
+        for (int i = 0; i < kDirectChains; ++i) {
+            const int k = min(k0 + i, n - 1);
+            acc[i] = first_mul ? __fmul_rn(x0, __ldg(t + k * n)) : x0;
+        }
+#pragma unroll 2
+        for (int j = 1; j < n; ++j) {
+            const float xj = in[j * kTP];
+#pragma unroll
+            for (int i = 0; i < kDirectChains; ++i) {
+                const int k = min(k0 + i, n - 1);
+                acc[i] = __fmaf_rn(xj, __ldg(t + k * n + j), acc[i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < kDirectChains; ++i)
+            if (k0 + i < n) out[k0 + i] = acc[i];
+    }
+}
+
 template <bool WIENER>
 __device__ __noinline__ float zstage_direct(float *Tc, const float *Wc, float t0, float t1, int n, const float *fwd,
                                             const float *inv)
 {
-    float x[32], X[32];
-    for (int j = 0; j < n; ++j) x[j] = Tc[j * kTP];
-    for (int k = 0; k < n; ++k) {
-        float acc = __fmul_rn(x[0], __ldg(fwd + k * n));
-        for (int j = 1; j < n; ++j) acc = __fmaf_rn(x[j], __ldg(fwd + k * n + j), acc);
-        X[k] = acc;
-    }
+    float X[32];
+    direct_sums(Tc, fwd, n, true, X);
     float r = 0.0f;
     if constexpr (!WIENER) {
         int kk = 0;
@@ -192,22 +218,21 @@ __device__ __noinline__ float zstage_direct(float *Tc, const float *Wc, float t0
             r = __fadd_rn(r, __fmul_rn(w, w));
         }
     }
-    for (int k = 0; k < n; ++k) {
-        float acc = X[0];
-        for (int j = 1; j < n; ++j) acc = __fmaf_rn(X[j], __ldg(inv + k * n + j), acc);
-        Tc[k * kTP] = acc;
-    }
+    // the spectrum goes back into the column, the inverse reads it from there
+    for (int zz = 0; zz < n; ++zz) Tc[zz * kTP] = X[zz];
+    float Y[32];
+    direct_sums(Tc, inv, n, false, Y);
+    for (int k = 0; k < n; ++k) Tc[k * kTP] = Y[k];
     return r;
 }
 
+// Wiener weights of a column of length n < G (direct sums as above), written back in place.
 __device__ __noinline__ void wiener_direct(float *Wc, float sg, int n, const float *fwd)
 {
-    float x[32];
-    for (int j = 0; j < n; ++j) x[j] = Wc[j * kTP];
+    float X[32];
+    direct_sums(Wc, fwd, n, true, X);
     for (int k = 0; k < n; ++k) {
-        float acc = __fmul_rn(x[0], __ldg(fwd + k * n));
-        for (int j = 1; j < n; ++j) acc = __fmaf_rn(x[j], __ldg(fwd + k * n + j), acc);
-        const float r2 = __fmul_rn(acc, acc);
+        const float r2 = __fmul_rn(X[k], X[k]);
         Wc[k * kTP] = __fdiv_rn(r2, __fadd_rn(r2, sg));
     }
 }

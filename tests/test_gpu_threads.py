@@ -58,4 +58,5 @@ def test_vbasic_two_threads():
 
     whole = make().numpy()
     split = _run_threads(make, [(0, 3), (3, 3)])
-    assert np.abs(split - whole).max() <= 1e-5
+    # 16-bit output: the float sums before the rounding differ in their last bits at most
+    assert np.abs(split.astype(np.int64) - whole.astype(np.int64)).max() <= 1

@@ -316,12 +316,18 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
     float *T2 = T + 32 * kTP;
 
     const long long nwarps = (long long)gridDim.x * nwarp;
-    // with a partial-group list the warps walk the list (one group per slot), else every group
-    const long long nitems = a.plist ? (long long)*a.plist_n : a.ngroups;
+    // with a partial-group list the warps walk the list, else every group.  With one group per
+    // warp, each plane of a listed group is a slot of its own: the list is short (the groups the
+    // tensor-core kernel left) and its groups are slow (direct sums of any length), so three
+    // times the warps share it.
+    constexpr bool kPlaneSlots = GPW == 1;
+    const bool split = a.plist && kPlaneSlots;
+    const long long nitems = a.plist ? (long long)*a.plist_n * (split ? 3 : 1) : a.ngroups;
     for (long long wg = (long long)blockIdx.x * nwarp + warp; wg * GPW < nitems; wg += nwarps) {
         const long long item = wg * GPW + sub;
         const bool inrange = item < nitems;
-        const long long grp = a.plist ? (inrange ? a.plist[item] : 0) : item;
+        const int pslot = split ? (int)(item % 3) : -1;
+        const long long grp = a.plist ? (inrange ? a.plist[split ? item / 3 : item] : 0) : item;
         const long long g0 = inrange ? grp : 0;
         const int n = min(a.count[g0], G);
         // skip_full: full groups were filtered by the tensor-core kernel; only partial ones here
@@ -331,7 +337,7 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
         const bool full = __all_sync(0xffffffffu, n == G);
         const uint32_t pk = a.pos[g0 * G + min(z, n - 1)];
         for (int p = 0; p < 3; ++p) {
-            if (!a.process[p]) continue;
+            if (!a.process[p] || (pslot >= 0 && p != pslot)) continue;
             const GroupLoc L = locate(a, p, g0, pk);
             float blk[64];
             if constexpr (WIENER) {

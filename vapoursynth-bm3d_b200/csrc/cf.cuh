@@ -169,38 +169,48 @@ __device__ __noinline__ void wiener_column(float *Wc, float sg)
 // of the inverse) are touched O(n) times only.
 constexpr int kDirectChains = 8;
 
-// out[k] = sum_j t[k][j] x[j] for k < n, x[j] = in[j * kTP]; first term a product, as above
-__device__ __forceinline__ void direct_sums(const float *in, const float *t, int n, bool first_mul, float *out)
+// out_c[k] = sum_j t[k][j] x_c[j] for k < n and the two columns c of a lane, x_c[j] = in_c[j * kTP];
+// the first term a product (forward tables) or the bare x_c[0] (inverse tables, t[k][0] = 1).
+// Each table entry is loaded once for both columns.
+__device__ __forceinline__ void direct_sums2(const float *in0, const float *in1, const float *t, int n, bool first_mul,
+                                             float *out0, float *out1)
 {
     for (int k0 = 0; k0 < n; k0 += kDirectChains) {
-        float acc[kDirectChains];
-        const float x0 = in[0];
+        const float *tk[kDirectChains];
+#pragma unroll
+        for (int i = 0; i < kDirectChains; ++i) tk[i] = t + min(k0 + i, n - 1) * n;
+        float a0[kDirectChains], a1[kDirectChains];
+        const float x0 = in0[0], y0 = in1[0];
 #pragma unroll
         for (int i = 0; i < kDirectChains; ++i) {
-            const int k = min(k0 + i, n - 1);
-            acc[i] = first_mul ? __fmul_rn(x0, __ldg(t + k * n)) : x0;
+            const float f = first_mul ? __ldg(tk[i]) : 1.0f;
+            a0[i] = first_mul ? __fmul_rn(x0, f) : x0;
+            a1[i] = first_mul ? __fmul_rn(y0, f) : y0;
         }
 #pragma unroll 2
         for (int j = 1; j < n; ++j) {
-            const float xj = in[j * kTP];
+            const float xj = in0[j * kTP], yj = in1[j * kTP];
 #pragma unroll
             for (int i = 0; i < kDirectChains; ++i) {
-                const int k = min(k0 + i, n - 1);
-                acc[i] = __fmaf_rn(xj, __ldg(t + k * n + j), acc[i]);
+                const float f = __ldg(tk[i] + j);
+                a0[i] = __fmaf_rn(xj, f, a0[i]);
+                a1[i] = __fmaf_rn(yj, f, a1[i]);
             }
         }
 #pragma unroll
         for (int i = 0; i < kDirectChains; ++i)
-            if (k0 + i < n) out[k0 + i] = acc[i];
+            if (k0 + i < n) {
+                out0[k0 + i] = a0[i];
+                out1[k0 + i] = a1[i];
+            }
     }
 }
 
+// hard threshold (t0: kz = 0, t1: the rest) or Wiener weights (W) of a spectrum of length n;
+// returns the kept count or the sum of the squared weights, accumulated in kz order
 template <bool WIENER>
-__device__ __noinline__ float zstage_direct(float *Tc, const float *Wc, float t0, float t1, int n, const float *fwd,
-                                            const float *inv)
+__device__ __forceinline__ float shrink_direct(float *X, const float *W, float t0, float t1, int n)
 {
-    float X[32];
-    direct_sums(Tc, fwd, n, true, X);
     float r = 0.0f;
     if constexpr (!WIENER) {
         int kk = 0;
@@ -213,28 +223,53 @@ __device__ __noinline__ float zstage_direct(float *Tc, const float *Wc, float t0
         r = (float)kk;
     } else {
         for (int zz = 0; zz < n; ++zz) {
-            const float w = Wc[zz * kTP];
+            const float w = W[zz * kTP];
             X[zz] = __fmul_rn(X[zz], w);
             r = __fadd_rn(r, __fmul_rn(w, w));
         }
     }
-    // the spectrum goes back into the column, the inverse reads it from there
-    for (int zz = 0; zz < n; ++zz) Tc[zz * kTP] = X[zz];
-    float Y[32];
-    direct_sums(Tc, inv, n, false, Y);
-    for (int k = 0; k < n; ++k) Tc[k * kTP] = Y[k];
     return r;
 }
 
-// Wiener weights of a column of length n < G (direct sums as above), written back in place.
-__device__ __noinline__ void wiener_direct(float *Wc, float sg, int n, const float *fwd)
+// the z stage of two columns of length n < G (forward, shrinkage, inverse; results in place);
+// r[c] as shrink_direct's
+template <bool WIENER>
+__device__ __noinline__ void zstage_direct2(float *T0, float *T1, const float *W0, const float *W1, float t00, float t10,
+                                            float t01, float t11, int n, const float *fwd, const float *inv, float *r)
 {
-    float X[32];
-    direct_sums(Wc, fwd, n, true, X);
-    for (int k = 0; k < n; ++k) {
-        const float r2 = __fmul_rn(X[k], X[k]);
-        Wc[k * kTP] = __fdiv_rn(r2, __fadd_rn(r2, sg));
+    float X0[32], X1[32];
+    direct_sums2(T0, T1, fwd, n, true, X0, X1);
+    r[0] = shrink_direct<WIENER>(X0, W0, t00, t10, n);
+    r[1] = shrink_direct<WIENER>(X1, W1, t01, t11, n);
+    // the spectra go back into the columns, the inverse reads them from there
+    for (int zz = 0; zz < n; ++zz) {
+        T0[zz * kTP] = X0[zz];
+        T1[zz * kTP] = X1[zz];
     }
+    direct_sums2(T0, T1, inv, n, false, X0, X1);
+    for (int k = 0; k < n; ++k) {
+        T0[k * kTP] = X0[k];
+        T1[k * kTP] = X1[k];
+    }
+}
+
+// Wiener weights of two columns of length n < G (direct sums as above), written back in place
+__device__ __noinline__ void wiener_direct2(float *W0, float *W1, float sg, int n, const float *fwd)
+{
+    float X0[32], X1[32];
+    direct_sums2(W0, W1, fwd, n, true, X0, X1);
+    for (int k = 0; k < n; ++k) {
+        const float r0 = __fmul_rn(X0[k], X0[k]), r1 = __fmul_rn(X1[k], X1[k]);
+        W0[k * kTP] = __fdiv_rn(r0, __fadd_rn(r0, sg));
+        W1[k * kTP] = __fdiv_rn(r1, __fadd_rn(r1, sg));
+    }
+}
+
+// lengths the unrolled column transforms handle; the rest take the direct sums
+template <int G>
+__device__ __forceinline__ bool direct_length(int n)
+{
+    return !(n == G || (G > 16 && n == 16) || (G > 8 && n == 8) || n == 4 || n == 2 || n == 1);
 }
 
 template <int G, bool WIENER>
@@ -246,8 +281,7 @@ __device__ __forceinline__ float zstage_any(float *Tc, const float *Wc, float t0
     if (G > 8 && n == 8) return zstage_column<(G > 8 ? 8 : 1), WIENER>(Tc, Wc, t0, t1);
     if (n == 4) return zstage_column<4, WIENER>(Tc, Wc, t0, t1);
     if (n == 2) return zstage_column<2, WIENER>(Tc, Wc, t0, t1);
-    if (n == 1) return zstage_column<1, WIENER>(Tc, Wc, t0, t1);
-    return zstage_direct<WIENER>(Tc, Wc, t0, t1, n, fwd, inv);
+    return zstage_column<1, WIENER>(Tc, Wc, t0, t1);   // n == 1 (direct lengths go in pairs)
 }
 
 template <int G>
@@ -258,8 +292,7 @@ __device__ __forceinline__ void wiener_any(float *Wc, float sg, int n, const flo
     else if (G > 8 && n == 8) wiener_column<(G > 8 ? 8 : 1)>(Wc, sg);
     else if (n == 4) wiener_column<4>(Wc, sg);
     else if (n == 2) wiener_column<2>(Wc, sg);
-    else if (n == 1) wiener_column<1>(Wc, sg);
-    else wiener_direct(Wc, sg, n, fwd);
+    else wiener_column<1>(Wc, sg);   // n == 1 (direct lengths go in pairs)
 }
 
 __device__ __forceinline__ const float *dtab_for(const CFArgs &a, int N, bool inverse)
@@ -363,8 +396,14 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
                     }
                 } else {
                     const float *fwd = n == G ? nullptr : dtab_for(a, n, false);
+                    if (direct_length<G>(n)) {
 #pragma unroll 1
-                    for (int q = 0; q < C; ++q) wiener_any<G>(T2 + sub * G * kTP + z + q * G, sg, n, fwd);
+                        for (int q = 0; q < C; q += 2)
+                            wiener_direct2(T2 + sub * G * kTP + z + q * G, T2 + sub * G * kTP + z + (q + 1) * G, sg, n, fwd);
+                    } else {
+#pragma unroll 1
+                        for (int q = 0; q < C; ++q) wiener_any<G>(T2 + sub * G * kTP + z + q * G, sg, n, fwd);
+                    }
                 }
                 __syncwarp();
             }
@@ -411,16 +450,34 @@ __global__ void __launch_bounds__(128) cf_fast_kernel(CFArgs a)
             } else {
                 const float *fwd = dtab_for(a, n, false);
                 const float *inv = dtab_for(a, n, true);
+                if (direct_length<G>(n)) {
+                    // a length without an unrolled transform: the direct sums, two columns at a time
 #pragma unroll 1
-                for (int q = 0; q < C; ++q) {
-                    const int c = z + q * G;
-                    const int fxy = ((c & 7) == 0) + ((c >> 3) == 0);
-                    const float t0 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy + 1];
-                    const float t1 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy];
-                    const float r = zstage_any<G, WIENER>(T + sub * G * kTP + c, WIENER ? T2 + sub * G * kTP + c : nullptr,
-                                                          t0, t1, n, n == G ? nullptr : fwd, n == G ? nullptr : inv);
-                    if constexpr (!WIENER) kept += (int)r;
-                    else l2 = __fadd_rn(l2, r);
+                    for (int q = 0; q < C; q += 2) {
+                        const int ca = z + q * G, cb = ca + G;
+                        const int fa = ((ca & 7) == 0) + ((ca >> 3) == 0), fb = ((cb & 7) == 0) + ((cb >> 3) == 0);
+                        float r[2];
+                        float *c0 = T + sub * G * kTP + ca;
+                        const float *w0 = WIENER ? T2 + sub * G * kTP + ca : nullptr;
+                        zstage_direct2<WIENER>(c0, c0 + G, w0, WIENER ? w0 + G : nullptr,
+                                               WIENER ? 0.0f : a.thr4[p][n - 1][fa + 1], WIENER ? 0.0f : a.thr4[p][n - 1][fa],
+                                               WIENER ? 0.0f : a.thr4[p][n - 1][fb + 1], WIENER ? 0.0f : a.thr4[p][n - 1][fb],
+                                               n, fwd, inv, r);
+                        if constexpr (!WIENER) kept += (int)r[0] + (int)r[1];
+                        else l2 = __fadd_rn(__fadd_rn(l2, r[0]), r[1]);
+                    }
+                } else {
+#pragma unroll 1
+                    for (int q = 0; q < C; ++q) {
+                        const int c = z + q * G;
+                        const int fxy = ((c & 7) == 0) + ((c >> 3) == 0);
+                        const float t0 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy + 1];
+                        const float t1 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy];
+                        const float r = zstage_any<G, WIENER>(T + sub * G * kTP + c, WIENER ? T2 + sub * G * kTP + c : nullptr,
+                                                              t0, t1, n, nullptr, nullptr);
+                        if constexpr (!WIENER) kept += (int)r;
+                        else l2 = __fadd_rn(l2, r);
+                    }
                 }
             }
 #pragma unroll
@@ -598,8 +655,14 @@ __global__ void __launch_bounds__(kCfWarps * 32, 1) cf_run_kernel(CFArgs a)
                         }
                     } else {
                         const float *fwd = n == G ? nullptr : dtab_for(a, n, false);
-    #pragma unroll 1
-                        for (int q = 0; q < C; ++q) wiener_any<G>(T2 + sub * G * kTP + z + q * G, sg, n, fwd);
+                        if (direct_length<G>(n)) {
+#pragma unroll 1
+                            for (int q = 0; q < C; q += 2)
+                                wiener_direct2(T2 + sub * G * kTP + z + q * G, T2 + sub * G * kTP + z + (q + 1) * G, sg, n, fwd);
+                        } else {
+#pragma unroll 1
+                            for (int q = 0; q < C; ++q) wiener_any<G>(T2 + sub * G * kTP + z + q * G, sg, n, fwd);
+                        }
                     }
                     __syncwarp();
                 }
@@ -646,16 +709,34 @@ __global__ void __launch_bounds__(kCfWarps * 32, 1) cf_run_kernel(CFArgs a)
                 } else {
                     const float *fwd = dtab_for(a, n, false);
                     const float *inv = dtab_for(a, n, true);
-    #pragma unroll 1
-                    for (int q = 0; q < C; ++q) {
-                        const int c = z + q * G;
-                        const int fxy = ((c & 7) == 0) + ((c >> 3) == 0);
-                        const float t0 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy + 1];
-                        const float t1 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy];
-                        const float r = zstage_any<G, WIENER>(T + sub * G * kTP + c, WIENER ? T2 + sub * G * kTP + c : nullptr,
-                                                              t0, t1, n, n == G ? nullptr : fwd, n == G ? nullptr : inv);
-                        if constexpr (!WIENER) kept += (int)r;
-                        else l2 = __fadd_rn(l2, r);
+                    if (direct_length<G>(n)) {
+                        // a length without an unrolled transform: the direct sums, two columns at a time
+#pragma unroll 1
+                        for (int q = 0; q < C; q += 2) {
+                            const int ca = z + q * G, cb = ca + G;
+                            const int fa = ((ca & 7) == 0) + ((ca >> 3) == 0), fb = ((cb & 7) == 0) + ((cb >> 3) == 0);
+                            float r[2];
+                            float *c0 = T + sub * G * kTP + ca;
+                            const float *w0 = WIENER ? T2 + sub * G * kTP + ca : nullptr;
+                            zstage_direct2<WIENER>(c0, c0 + G, w0, WIENER ? w0 + G : nullptr,
+                                                   WIENER ? 0.0f : a.thr4[p][n - 1][fa + 1], WIENER ? 0.0f : a.thr4[p][n - 1][fa],
+                                                   WIENER ? 0.0f : a.thr4[p][n - 1][fb + 1], WIENER ? 0.0f : a.thr4[p][n - 1][fb],
+                                                   n, fwd, inv, r);
+                            if constexpr (!WIENER) kept += (int)r[0] + (int)r[1];
+                            else l2 = __fadd_rn(__fadd_rn(l2, r[0]), r[1]);
+                        }
+                    } else {
+#pragma unroll 1
+                        for (int q = 0; q < C; ++q) {
+                            const int c = z + q * G;
+                            const int fxy = ((c & 7) == 0) + ((c >> 3) == 0);
+                            const float t0 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy + 1];
+                            const float t1 = WIENER ? 0.0f : a.thr4[p][n - 1][fxy];
+                            const float r = zstage_any<G, WIENER>(T + sub * G * kTP + c, WIENER ? T2 + sub * G * kTP + c : nullptr,
+                                                                  t0, t1, n, nullptr, nullptr);
+                            if constexpr (!WIENER) kept += (int)r;
+                            else l2 = __fadd_rn(l2, r);
+                        }
                     }
                 }
     #pragma unroll

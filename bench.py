@@ -7,8 +7,9 @@ Workload (one step): 8 synthetic RGB float32 1920x1080 frames per GPU through
 the full-pipeline configuration of the reference plugin's benchmark (8 frames, 1080p RGB).
 Four forms run: the plain FP32 path (precision="fp32", the oracle-exact drop-in), the precision
 form (precision="tf32": tensor-core transforms, tensor-core matching estimates with exact
-re-rank), the same with Basic at precision="fp32" ("tf32_final": the hard-threshold filter keeps
-the plain transform, the Final one runs on the tensor cores) and the learned-proposal form
+re-rank), the same with Basic at precision="tf32_match" ("tf32_final": Basic's matching on the
+tensor cores but its hard-threshold filter on the plain transform, the Final filter on the tensor
+cores) and the learned-proposal form
 (precision="learned": as tf32, but matching re-ranks only the proposals of the learned descriptor
 network).  `value` is the fastest of the tensor-core forms whose output PSNR against the clean
 frames stays within 0.05 dB of the plain path's (else the plain path's); `forms` gives all four.  `value` times the device-resident pipeline (frames
@@ -309,9 +310,9 @@ def ours_arm(args):
     stream = torch.cuda.Stream()
     vi = capi.VideoInfo(capi.RGB, capi.FLOAT, 32, 0, 0, Wd, Hd, F)
     # forms: the plain drop-in; tensor cores in both filters; the hard-threshold filter in FP32
-    # (exact decisions, and faster than its tensor-core version) with the tensor-core Final; and
-    # the learned proposals
-    precisions = {"fp32": "fp32", "tf32": "tf32", "tf32_final": ("fp32", "tf32"), "learned": "learned"}
+    # (exact decisions, and faster than its tensor-core version) after tensor-core matching, with
+    # the tensor-core Final; and the learned proposals
+    precisions = {"fp32": "fp32", "tf32": "tf32", "tf32_final": ("tf32_match", "tf32"), "learned": "learned"}
     pipes = {form: Pipeline(L, capi, vi, stream, pr) for form, pr in precisions.items()}
 
     def planes(n):

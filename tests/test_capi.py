@@ -82,8 +82,8 @@ ERRORS = [
     ("Basic", dict(input=clip(cf=bm3d_b200.YUV), matrix=3), "bm3d.Basic: Unsupported \"matrix\" specified"),
     ("Basic", dict(input=clip(cf=bm3d_b200.YUV, ssw=1, ssh=1)), "bm3d.Basic: input clip: sub-sampled format is not supported when chroma is processed, convert it to YUV444 or RGB first. For the best quality, RGB colorspace is recommended as input."),
     ("Basic", dict(input=clip(), hard_thr=0.0), "bm3d.Basic: Invalid \"hard_thr\" assigned, must be a positive floating point number"),
-    ("Basic", dict(input=clip(), precision="fp16"), "bm3d.Basic: Invalid \"precision\" assigned, must be \"fp32\", \"tf32\" or \"learned\""),
-    ("VFinal", dict(input=clip(), ref=clip(), precision="bf16"), "bm3d.VFinal: Invalid \"precision\" assigned, must be \"fp32\", \"tf32\" or \"learned\""),
+    ("Basic", dict(input=clip(), precision="fp16"), "bm3d.Basic: Invalid \"precision\" assigned, must be \"fp32\", \"tf32\", \"tf32_match\" or \"learned\""),
+    ("VFinal", dict(input=clip(), ref=clip(), precision="bf16"), "bm3d.VFinal: Invalid \"precision\" assigned, must be \"fp32\", \"tf32\", \"tf32_match\" or \"learned\""),
     ("VBasic", dict(input=clip(), aggregate=2), "bm3d.VBasic: Invalid \"aggregate\" assigned, must be 0 (stacked output) or 1 (aggregated output)"),
     ("VFinal", dict(input=clip(), ref=clip(), aggregate=1, sample=2), "bm3d.VFinal: Invalid 'sample' assigned, must be 0 (integer sample type) or 1 (float sample type)"),
     ("Final", dict(input=clip(), ref=clip(), group_size=0), "bm3d.Final: Invalid \"group_size\" assigned, must be an integer in [1, 256]"),

@@ -163,3 +163,48 @@ def test_precision_form_2160p(sigma):
     # flips against exact arithmetic (about 1e-8 of the decisions at 1080p)
     decisions = 4 * res["fp32"]["b"].retained_counts(0).shape[1] * 16 * 64
     assert fl <= 1e-7 * decisions
+
+
+def test_tf32_final_short_groups():
+    """Final on the tensor cores when most groups are shorter than group_size (a small th_mse
+    leaves few candidates under the distance threshold): a short group takes the transforms of
+    its own length in its rows of the z-stage matrices.  Against the plain Final (same Basic
+    estimate as ref): PSNR within 0.05 dB and max deviation 2e-3 (the Wiener filter has no
+    keep / zero decisions, so only tf32 rounding separates the two)."""
+    sigma = 20.0
+    nz, clean = synth.gray_frames(56, 2, 160, 224, sigma)
+    clip = source(nz, "GRAY")
+    basic = core.bm3d.Basic(clip, profile="np", sigma=sigma).numpy()
+    out, short = {}, {}
+    for prec in ("fp32", "tf32"):
+        node = core.bm3d.Final(clip, source(basic, "GRAY"), profile="np", sigma=sigma,
+                               th_mse=100.0, precision=prec)
+        out[prec] = node.numpy()
+        cnt = node.matches(0, 32)[0]
+        short[prec] = float(np.mean(cnt < 32))
+    assert short["tf32"] == short["fp32"]          # the same lists
+    print(f"short groups: {short['tf32']:.3f}")
+    assert short["tf32"] > 0.5
+    check_close(out["tf32"], out["fp32"], clean, sigma, "final, short groups")
+    assert float(np.abs(out["tf32"].astype(np.float64) - out["fp32"]).max()) <= 2e-3
+
+
+def test_tf32_match_output_is_plain():
+    """precision="tf32_match": the tensor-core matching (the plain kernel's lists) with the plain
+    transforms, so Basic and Final give the "fp32" output up to the order of the aggregation's
+    float atomics (which makes the plain path itself vary in the last bits): lists identical,
+    outputs within 1e-5.  Both Finals take the same ref (a last-bit difference of the ref can
+    reorder near-equal candidates)."""
+    nz, _ = synth.gray_frames(57, 2, 144, 176, 10.0)
+    clip = source(nz, "GRAY")
+    ref = source(core.bm3d.Basic(clip, profile="np", sigma=10.0).numpy(), "GRAY")
+    out, lists = {}, {}
+    for prec in ("fp32", "tf32_match"):
+        basic = core.bm3d.Basic(clip, profile="np", sigma=10.0, precision=prec)
+        final = core.bm3d.Final(clip, ref, profile="np", sigma=10.0, precision=prec)
+        out[prec] = (basic.numpy(), final.numpy())
+        lists[prec] = basic.matches(0, 16)[:4] + final.matches(0, 32)[:4]
+    for u, v in zip(lists["tf32_match"], lists["fp32"]):
+        assert np.array_equal(u, v)
+    for u, v in zip(out["tf32_match"], out["fp32"]):
+        assert float(np.abs(u.astype(np.float64) - v).max()) <= 1e-5

@@ -4,8 +4,10 @@
 // Same arithmetic contract as cf_fast_kernel (source/BM3D_Basic.cpp:72-148,
 // source/BM3D_Final.cpp:50-127, aggregation include/Block.h:1239-1387) except that the transforms
 // are dense matrix products with tf32 operands, so coefficients carry ~2^-11 relative error: the
-// output is close to, not bit-identical with, the plain FP32 path.  Only full groups (n == G) are
-// handled here; the plain kernel filters the partial ones in the same pass over the match lists.
+// output is close to, not bit-identical with, the plain FP32 path.  The hard-threshold kernels
+// handle full groups (n == G) only, and the plain kernel filters the partial ones afterwards; the
+// Wiener kernels with G = 16 / 32 filter every group, a short one (n < G) with the n-point
+// transforms in its rows of the z-stage matrices.
 //
 // A tile is 128 blocks = 128 / G groups of one plane, handled by one warpgroup (128 threads);
 // thread r owns row r = block (r % G) of group r / G.  A CTA runs several warpgroups, each on its
@@ -78,6 +80,13 @@ struct TcShape {
     static constexpr bool kZInTmem = kWG == 2 && G >= 16;
     static constexpr int kTmemCols = kWG == 4 ? 512 : (kZInTmem ? 512 : 256);
     static constexpr int kZCol = 128 * kWG;              // first column of the stacks
+    // Wiener filter with the stacks in tensor memory: groups of fewer than G blocks are filtered
+    // here too.  A tile holding one gets its own stacks (per team, after the shared ones) whose
+    // rows of group w are the n_w-point matrices (zero past n_w), so each group's z products are
+    // its own length's transforms.
+    static constexpr bool kShort = WIENER && kZInTmem;
+    static constexpr int kPCol = kZCol + 2 * G;
+    static_assert(!kShort || kPCol + kWG * 2 * G <= kTmemCols, "tensor memory: per-team stacks do not fit");
     static constexpr int kTabOff = kZInTmem ? TcLayout<G>::kKf : 0;   // first table byte kept in shared memory
     // Image boxes of the region mode: Final with the stacks in tensor memory keeps a source box,
     // a reference box and the aggregation box, so that the next plane's boxes load while this
@@ -268,6 +277,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     // output lane disabled; Bt swizzled [nt rows][128 k]
     // The per-group chains are independent (disjoint output lanes), so consecutive products go
     // to different groups: K step outer, group inner.
+    uint32_t zcol = Shp::kZCol;                      // first column of the stacks the z products read
     auto z_stage = [&](uint32_t d0, uint32_t sz, int nt, uint32_t idesc) {
 #pragma unroll 1
         for (int s = 0; s < G / 8; ++s) {
@@ -285,7 +295,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 const uint32_t k0 = (uint32_t)(G * w + 8 * s);
                 const uint64_t bd = tc::make_desc_sw128(sD + (k0 / 32) * (nt / 8) * 1024 + ((k0 % 32) / 8) * 32, 1024);
                 if constexpr (Shp::kZInTmem)
-                    tc::mma_ts_tf32_masked(tb + d0, tm + Shp::kZCol + (sz == sZi ? G : 0) + 8 * s, bd, idesc, s > 0,
+                    tc::mma_ts_tf32_masked(tb + d0, tm + zcol + (sz == sZi ? G : 0) + 8 * s, bd, idesc, s > 0,
                                            m[0], m[1], m[2], m[3]);
                 else
                     tc::mma_ss_tf32_masked(tb + d0, ad, bd, idesc, s > 0, m[0], m[1], m[2], m[3]);
@@ -322,7 +332,9 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
         const long long grp = tl * GPT + wsub;
         const bool inrange = tl < ntiles && grp < a.ngroups;
         T.g0 = inrange ? grp : 0;
-        T.mine = inrange && a.count[T.g0] >= G;       // full group: filtered here
+        const int cnt = inrange ? a.count[T.g0] : 0;
+        // full groups are filtered here; with kShort every group, block j if j < its count
+        T.mine = inrange && (Shp::kShort ? j < cnt : cnt >= G);
         T.pk = a.pos[T.g0 * G + j];
         T.region = false;
         T.y0 = T.x0 = T.rh = T.rw = T.rp = T.frame = 0;
@@ -393,6 +405,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     // Ci[b][0] = 1, Ci[b][kz] = Dz[kz][b]): a warp's lanes read consecutive words
     const float *dzt = reinterpret_cast<const float *>(xtab + 64 + G * G);
     const float *dzi = dzt + G * G;
+    // then (kShort) the rows of the n-point stacks, n = 1 .. G: [n - 1][forward, inverse][row][G]
+    const float *ztn = dzi + G * G;
     unsigned long long n_recheck = 0, n_changed = 0;
 
     bool failed = false;
@@ -409,6 +423,28 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
         const uint32_t pk = cur.pk;
         const bool region = cur.region;
         const int y0 = cur.y0, x0 = cur.x0, rh = cur.rh, rw = cur.rw, rp = cur.rp, frame = cur.frame;
+        // blocks in this row's group (rows past the last group read group 0's count: unused)
+        auto group_n = [&]() { return Shp::kShort ? min(max(a.count[g0], 1), G) : G; };
+        if constexpr (Shp::kShort) {
+            // a tile with a short group: this team's stacks get each group's own matrices (the
+            // previous tile's products have completed: every product is waited for)
+            const int gn = group_n();
+            const bool tpart = !tc::wg_and(bar_id, TEAM, gn == G);
+            zcol = tpart ? (uint32_t)(Shp::kPCol + wg * 2 * G) : (uint32_t)Shp::kZCol;
+            if (tpart && t < 128) {
+                const float *zr = ztn + (size_t)(gn - 1) * 2 * G * G + (size_t)j * G;
+#pragma unroll
+                for (int m = 0; m < 2; ++m)
+#pragma unroll
+                    for (int k0 = 0; k0 < G; k0 += 16) {
+                        float v[16];
+#pragma unroll
+                        for (int e = 0; e < 16; ++e) v[e] = __ldg(zr + m * G * G + k0 + e);
+                        tc::tmem_st16(tm + lrow + zcol + m * G + k0, v);
+                    }
+                tc::tmem_wait_st();
+            }
+        }
         for (int p = 0; p < 3 && !failed; ++p) {
             if (!a.process[p]) continue;
             const GroupLoc L = locate(a, p, g0, pk);
@@ -466,7 +502,9 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         for (int k = 0; k < 4; ++k) {
                             const int i = i0 + k;
                             const bool g1 = GW > 1 && b0 + i - gfirst >= G;
-                            const float ms = g1 ? lv[2] : lv[0], mr = g1 ? lv[3] : lv[1];
+                            // rows past a short group's count stay zero
+                            const bool mi = pq[k] >= 0;
+                            const float ms = mi ? (g1 ? lv[2] : lv[0]) : 0.f, mr = mi ? (g1 ? lv[3] : lv[1]) : 0.f;
                             *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane, 128)) = v0[k] - ms;
                             *reinterpret_cast<float *>(D + tc::sw128_offset(b0 + i, lane + 32, 128)) = v1[k] - ms;
                             *reinterpret_cast<float *>(D + Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128)) = u0[k] - mr;
@@ -598,6 +636,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 // each lane re-reads only the elements its own copies wrote
 #pragma unroll 4
                 for (int i = half * NI; i < half * NI + NI; ++i) {
+                    // (kShort) rows past a short group's count stay zero
+                    if (Shp::kShort && !__shfl_sync(0xffffffffu, mine, i)) continue;
 #pragma unroll
                     for (int op = 0; op < (WIENER ? 2 : 1); ++op) {
                         float *d0 = reinterpret_cast<float *>(D + op * Lay::kXBytes + tc::sw128_offset(b0 + i, lane, 128));
@@ -650,6 +690,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             if (!wait_mma()) { failed = true; break; }
             // 5. shrinkage, one row of 64 coefficients per thread
             float acc = 0.0f;
+            const int gn = group_n();
             float thr[3];                              // by the number of zero (y, x) frequencies
 #pragma unroll
             for (int k = 0; k < 3; ++k) thr[k] = WIENER ? 0.0f : a.thr4[p][G - 1][(j == 0) + k];
@@ -660,8 +701,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             if constexpr (WIENER) {
                 // the group's levels: sum_b Dz[0][b] = 2 G, sum_b Dz[kz][b] = 0 for kz > 0
                 if (half == 0 && j == 0) {
-                    dcz = my_mu * (float)(2 * G);
-                    dczr = my_mur * (float)(2 * G);
+                    dcz = my_mu * (float)(2 * gn);
+                    dczr = my_mur * (float)(2 * gn);
                 }
             } else if constexpr (SPLIT >= 2) {
                 if (half == 0) {
@@ -705,7 +746,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         z[0] += dcz;
                         rr[0] += dczr;
                     }
-                    const float sg = a.wsig2[p][G - 1];
+                    const float sg = a.wsig2[p][gn - 1];
 #pragma unroll
                     for (int e = 0; e < 32; ++e) {
                         const float r2 = rr[e] * rr[e];
@@ -803,7 +844,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             } else {
                 denW = acc < 1.0f ? 1.0f : 1.0f / acc;
             }
-            const float numW = denW / a.amp[G - 1];
+            const float numW = denW / a.amp[gn - 1];
             publish();
             // (the barriers of the two inverse waits below order this before the aggregation)
             if constexpr (SPLIT >= 2) if (half == 0) part[r] = s00;

@@ -741,7 +741,8 @@ class BM3DBase : public Filter {
 public:
     bool wiener = false;
     bool vbm3d = false;
-    bool tc = false;            // precision form: tensor-core transforms (argument "precision")
+    bool tc = false;            // precision form: tensor-core matching estimates (argument "precision")
+    bool tc_cf = false;         // precision form: tensor-core transforms as well
     bool learned = false;       // precision "learned": block matching by learned proposals
     // extension of VBasic / VFinal: aggregate = 1 returns VAggregate(radius, sample) of the
     // filter's output directly, without the stacked clip
@@ -875,14 +876,16 @@ public:
             else if (para.lambda <= 0)
                 return fail(BM3D_ERR_ARG, err("Invalid \"hard_thr\" assigned, must be a positive floating point number"));
         }
-        // extension: "precision" selects the plain FP32 transforms ("fp32", default) or the
-        // tensor-core precision form ("tf32")
+        // extension: "precision" selects the plain FP32 path ("fp32", default), the tensor-core
+        // precision form ("tf32"), its matching alone with the plain transforms ("tf32_match":
+        // the same lists, so the output of "fp32") or the learned proposals ("learned")
         const char *prec = map_get_data(in, "precision", 0, &error);
         if (!error) {
             const std::string pr(prec);
-            if (pr == "tf32") tc = true;
-            else if (pr == "learned") tc = learned = true;
-            else if (pr != "fp32") return fail(BM3D_ERR_ARG, err("Invalid \"precision\" assigned, must be \"fp32\", \"tf32\" or \"learned\""));
+            if (pr == "tf32") tc = tc_cf = true;
+            else if (pr == "tf32_match") tc = true;
+            else if (pr == "learned") tc = tc_cf = learned = true;
+            else if (pr != "fp32") return fail(BM3D_ERR_ARG, err("Invalid \"precision\" assigned, must be \"fp32\", \"tf32\", \"tf32_match\" or \"learned\""));
         }
         if (vbm3d) {
             const int64_t ag = map_get_int64(in, "aggregate", 0, &error);
@@ -953,7 +956,7 @@ public:
         for (int n = 1; n <= para.G; ++n) lengths.push_back(n);
         lengths.push_back(para.B);
         build_direct_tables(dtabs, lengths);
-        if (tc && cf_tc_supported(para.B, para.G)) {
+        if (tc_cf && cf_tc_supported(para.B, para.G)) {
             std::vector<unsigned char> img;
             cf_tc_tables(para.G, img);
             // fp64 tables of the hard-threshold recheck after the image: C8[u][y], Dz[kz][b]
@@ -975,6 +978,10 @@ public:
                 for (int kz = 0; kz < para.G; ++kz) ft.push_back((float)dz[kz * para.G + b]);
             for (int kz = 0; kz < para.G; ++kz)
                 for (int b = 0; b < para.G; ++b) ft.push_back(kz == 0 ? 1.0f : (float)dz[kz * para.G + b]);
+            // then the rows of the n-point z-stage matrices (Wiener kernels, tiles with short groups)
+            std::vector<float> pt;
+            cf_tc_partial_tables(para.G, pt);
+            ft.insert(ft.end(), pt.begin(), pt.end());
             const size_t fbase = img.size();
             img.resize(fbase + ft.size() * sizeof(float));
             std::memcpy(img.data() + fbase, ft.data(), ft.size() * sizeof(float));
@@ -1243,7 +1250,9 @@ public:
             a.tc_stats = static_cast<unsigned long long *>(tc_counts.get(2 * sizeof(unsigned long long)));
             CU(cudaMemsetAsync(a.tc_stats, 0, 2 * sizeof(unsigned long long), stream));
             // precision form: full groups on the tensor cores, partial ones on the plain kernel
+            // unless the tensor-core kernel takes them too (Wiener filter, G = 16 / 32)
             CU(launch_cf_tc(a, tc_tab.p, tc_status.as<int>(), stream));
+            if (cf_tc_handles_partial(para.B, para.G, wiener)) return;
             a.skip_full = 1;
             // the plain kernel walks a list of the partial groups instead of skipping the full ones
             long long *pl = static_cast<long long *>(plist.get(sizeof(long long) * (size_t)std::max<long long>(1, ngroups)));

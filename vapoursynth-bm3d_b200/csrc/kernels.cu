@@ -242,6 +242,28 @@ static void tc_tables_t(std::vector<unsigned char> &img)
                 }
 }
 
+// Rows of the n-point z-stage matrices, n = 1 .. G, as the Wiener kernels load them into tensor
+// memory for tiles with a short group: [n - 1][forward, inverse][row j][G], forward row j = the
+// REDFT10 coefficients of frequency j, inverse row j = the REDFT01 coefficients of block j, zero
+// past n (rows and columns).
+void cf_tc_partial_tables(int G, std::vector<float> &out)
+{
+    out.assign((size_t)G * 2 * G * G, 0.0f);
+    for (int n = 1; n <= G; ++n)
+        for (int r = 0; r < n; ++r)
+            for (int k = 0; k < n; ++k) {
+                float *f = out.data() + (size_t)(n - 1) * 2 * G * G;
+                f[r * G + k] = round_tf32((float)cos2((long)(2 * k + 1) * r, 2L * n));
+                f[G * G + r * G + k] = round_tf32(k == 0 ? 1.0f : (float)cos2((long)k * (2 * r + 1), 2L * n));
+            }
+}
+
+int cf_tc_handles_partial(int B, int G, int wiener)
+{
+    if (!cf_tc_supported(B, G) || !wiener) return 0;
+    return G == 16 ? TcShape<16, true>::kShort : G == 32 ? TcShape<32, true>::kShort : TcShape<8, true>::kShort;
+}
+
 void cf_tc_tables(int G, std::vector<unsigned char> &img)
 {
     if (G == 8) tc_tables_t<8>(img);

@@ -60,6 +60,9 @@ int cf_fast_supported(int B, int G);
 // timed out.
 int cf_tc_supported(int B, int G);
 void cf_tc_tables(int G, std::vector<unsigned char> &img);
+void cf_tc_partial_tables(int G, std::vector<float> &out);
+// 1 if the tensor-core kernel for (B, G, wiener) also filters the groups of fewer than G blocks
+int cf_tc_handles_partial(int B, int G, int wiener);
 cudaError_t launch_cf_tc(const CFArgs &a, const void *tables, int *status, cudaStream_t s);
 
 // FP64 oracle of the collaborative filter, aggregation and normalisation for the groups of one

@@ -140,6 +140,9 @@ struct CFArgs {
     // device; the kernel then walks this list instead of every group
     const long long *plist;
     const unsigned int *plist_n;
+    // optional (tensor-core kernels): the tiles to filter, *tlist_n entries, instead of all
+    const int *tlist;
+    const unsigned int *tlist_n;
     // precision form, hard threshold: a coefficient whose tensor-core value lies within
     // recheck_band * thr of its threshold is recomputed in fp32 from the pixels before the keep /
     // zero decision (0 disables); tc_stats counts [0] coefficients recomputed, [1] decisions the

@@ -59,6 +59,10 @@ struct TcLayout {
     static constexpr int kKi = kKf + kKBytes;           // inverse 2-D matrix, [pixel][coef] (K-major)
     static constexpr int kTableBytes = kKi + kKBytes;
     static constexpr int kXBytes = 128 * 64 * 4;        // one 128 x 64 data operand
+    // image offset of the transposed form's z-stage matrices (after the fp64 tables, the fp32 DC
+    // tables and the n-point rows): Dz as [kz][b] and Ci as [b][kz], K-major, no swizzle
+    static constexpr int kZtOff = kTableBytes + (64 + G * G) * 8 + (2 * G * G + 2 * G * G * G) * 4;
+    static constexpr int kZtBytes = 2 * G * G * 4;
 };
 
 // Tile teams per CTA: shared memory holds the tables and, per team, one (Basic) or two (Final)
@@ -66,8 +70,13 @@ struct TcLayout {
 // 32-row quarter of the tile (kSplit = 1) or two (kSplit = 2: the two warps of a quarter share its
 // columns and gather / aggregation steps), so that the kernels limited to two teams by shared
 // memory (Final, and Basic with G = 32) still run 16 warps per SM.
-template <int G, bool WIENER>
+// ZT (Wiener filter, G = 32): the transposed z stage.  The z products put the coefficients of a
+// half tile on the tensor-memory lanes and the half's two groups on the columns, so each product
+// is the group's own 32-point transform (N = 32) instead of a 128-lane product with three
+// quarters of its lanes disabled: a quarter of the tensor work of the z stages.
+template <int G, bool WIENER, bool ZT = false>
 struct TcShape {
+    static_assert(!ZT || (WIENER && G == 32), "transposed z stage: Wiener filter with G = 32 only");
     static constexpr bool kTwo = WIENER || G == 32;     // two teams (shared memory), split quarters
     static constexpr int kWG = kTwo ? 2 : 4;
     static constexpr int kSplit = kTwo ? 2 : 1;
@@ -77,7 +86,7 @@ struct TcShape {
     // With two teams, tensor memory has room for the z-stage matrix stacks (G columns each): the
     // z products then read A from tensor memory and only B from shared memory, and the stacks
     // need no shared-memory copy.
-    static constexpr bool kZInTmem = kWG == 2 && G >= 16;
+    static constexpr bool kZInTmem = !ZT && kWG == 2 && G >= 16;
     static constexpr int kTmemCols = kWG == 4 ? 512 : (kZInTmem ? 512 : 256);
     static constexpr int kZCol = 128 * kWG;              // first column of the stacks
     // Wiener filter with the stacks in tensor memory: groups of fewer than G blocks are filtered
@@ -87,17 +96,20 @@ struct TcShape {
     static constexpr bool kShort = WIENER && kZInTmem;
     static constexpr int kPCol = kZCol + 2 * G;
     static_assert(!kShort || kPCol + kWG * 2 * G <= kTmemCols, "tensor memory: per-team stacks do not fit");
-    static constexpr int kTabOff = kZInTmem ? TcLayout<G>::kKf : 0;   // first table byte kept in shared memory
+    static constexpr int kTabOff = kZInTmem || ZT ? TcLayout<G>::kKf : 0;   // first table byte kept in shared memory
+    static constexpr int kZtBytes = ZT ? TcLayout<G>::kZtBytes : 0;   // (ZT) z-stage B operands after the tables
     // Image boxes of the region mode: Final with the stacks in tensor memory keeps a source box,
     // a reference box and the aggregation box, so that the next plane's boxes load while this
     // plane is filtered; otherwise one box serves the gathers and the aggregation in turn.
-    static constexpr int kBoxes = WIENER && kZInTmem ? 3 : 1;
+    static constexpr int kBoxes = WIENER && (kZInTmem || ZT) ? 3 : 1;
+    // (ZT) the aggregation box lives in the data region (its second half is free by then)
+    static constexpr int kBoxesExtra = ZT ? 2 : kBoxes;
     static constexpr int kRegion = kBoxes == 3 ? 2560 : 3072;   // floats per box
     // three-box form: a table of the tile's rows (block position in the box, weight) that the
     // block-step loops read with one broadcast load instead of three or four shuffles
     static constexpr int kRowTab = kBoxes == 3 ? 128 * 8 : 0;
-    static constexpr int kExtra = kPart + kRegion * 4 * kBoxes + 256 + kRowTab;   // + 2 x [4 quarters][8] ints of scratch
-    static constexpr int kSmem = (kData + kExtra) * kWG + TcLayout<G>::kTableBytes - kTabOff;
+    static constexpr int kExtra = kPart + kRegion * 4 * kBoxesExtra + 256 + kRowTab;   // + 2 x [4 quarters][8] ints of scratch
+    static constexpr int kSmem = (kData + kExtra) * kWG + TcLayout<G>::kTableBytes - kTabOff + kZtBytes;
 };
 
 // byte offset of element (row, k) of a K-major operand with `kdim` columns
@@ -149,12 +161,41 @@ __device__ __forceinline__ void block_means(float (&s)[N], int lane)
     }
 }
 
-template <int G, bool WIENER>
-__global__ void __launch_bounds__(TcShape<G, WIENER>::kTeam * TcShape<G, WIENER>::kWG, 1)
+// Tiles (128 / G consecutive groups) split into those whose groups are all full and those with
+// a short group, each list in ascending order within a warp's 32 tiles.
+__global__ void cf_tile_lists_kernel(const int *__restrict__ count, long long ngroups, int G, long long ntiles,
+                                     int *__restrict__ full, unsigned int *__restrict__ nfull,
+                                     int *__restrict__ shrt, unsigned int *__restrict__ nshort)
+{
+    const int lane = (int)(threadIdx.x & 31);
+    const int gpt = 128 / G;
+    for (long long t0 = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); t0 < ntiles;
+         t0 += (long long)gridDim.x * blockDim.x) {
+        const long long tl = t0 + lane;
+        bool all = true;
+        if (tl < ntiles)
+            for (int k = 0; k < gpt; ++k) {
+                const long long g = tl * gpt + k;
+                if (g < ngroups && count[g] < G) all = false;
+            }
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            const bool in = tl < ntiles && (l == 0 ? all : !all);
+            const unsigned m = __ballot_sync(0xffffffffu, in);
+            unsigned base = 0;
+            if (lane == 0 && m) base = atomicAdd(l == 0 ? nfull : nshort, (unsigned)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (in) (l == 0 ? full : shrt)[base + __popc(m & ((1u << lane) - 1u))] = (int)tl;
+        }
+    }
+}
+
+template <int G, bool WIENER, bool ZT = false>
+__global__ void __launch_bounds__(TcShape<G, WIENER, ZT>::kTeam * TcShape<G, WIENER, ZT>::kWG, 1)
 cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
 {
     using Lay = TcLayout<G>;
-    using Shp = TcShape<G, WIENER>;
+    using Shp = TcShape<G, WIENER, ZT>;
     constexpr int GPT = Lay::kGroups;
     constexpr int NWG = Shp::kWG;
     constexpr int SPLIT = Shp::kSplit;
@@ -179,19 +220,23 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     unsigned char *D = tsm + Shp::kData * wg;        // X | R, then Yt, then St
     unsigned char *extra = tsm + Shp::kData * NWG + Shp::kExtra * wg;
     float *part = reinterpret_cast<float *>(extra);
-    float *Rg = reinterpret_cast<float *>(extra + Shp::kPart);         // aggregation box
-    float *Bs = Shp::kBoxes == 3 ? Rg + Shp::kRegion : Rg;              // source box
-    float *Br = Shp::kBoxes == 3 ? Rg + 2 * Shp::kRegion : Rg;          // reference box
-    int *bbx = reinterpret_cast<int *>(extra + Shp::kPart + Shp::kRegion * 4 * Shp::kBoxes);   // [4 quarters][8]: maxima
+    float *boxes = reinterpret_cast<float *>(extra + Shp::kPart);
+    // aggregation box (ZT: in the second half of the data region, zeroed before each use)
+    float *Rg = ZT ? reinterpret_cast<float *>(D + Lay::kXBytes) : boxes;
+    float *Bs = Shp::kBoxes == 3 ? (ZT ? boxes : boxes + Shp::kRegion) : Rg;              // source box
+    float *Br = Shp::kBoxes == 3 ? (ZT ? boxes + Shp::kRegion : boxes + 2 * Shp::kRegion) : Rg;   // reference box
+    int *bbx = reinterpret_cast<int *>(extra + Shp::kPart + Shp::kRegion * 4 * Shp::kBoxesExtra);   // [4 quarters][8]: maxima
     int *bnd = bbx + 32;                                                  // [4 quarters][8]: tile bounds
     // [128]: (y - y0) << 16 | (x - x0) of the row's block in the box (-1: not this kernel's), numW bits
-    int2 *rowtab = reinterpret_cast<int2 *>(extra + Shp::kPart + Shp::kRegion * 4 * Shp::kBoxes + 256);
+    int2 *rowtab = reinterpret_cast<int2 *>(extra + Shp::kPart + Shp::kRegion * 4 * Shp::kBoxesExtra + 256);
     // table byte b lives at tab + b (b >= kTabOff)
     unsigned char *tab = tsm + (Shp::kData + Shp::kExtra) * NWG - Shp::kTabOff;
 
     for (int i = threadIdx.x; i < (Lay::kTableBytes - Shp::kTabOff) / 16; i += blockDim.x)
         reinterpret_cast<float4 *>(tab + Shp::kTabOff)[i] = tables[Shp::kTabOff / 16 + i];
-    if constexpr (Shp::kBoxes == 3)
+    for (int i = threadIdx.x; i < Shp::kZtBytes / 16; i += blockDim.x)
+        reinterpret_cast<float4 *>(tab + Lay::kTableBytes)[i] = tables[Lay::kZtOff / 16 + i];
+    if constexpr (Shp::kBoxes == 3 && !ZT)
         for (int i = t; i < Shp::kRegion; i += TEAM) Rg[i] = 0.0f;   // the aggregation box starts (and stays) zero
     if (warp == 0) tc::tmem_alloc(&tslot, Shp::kTmemCols);
     if (t == 0) {
@@ -231,6 +276,9 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     const uint32_t sKf = tc::smem_u32(tab + Lay::kKf), sKi = tc::smem_u32(tab + Lay::kKi);
     const uint32_t sD = tc::smem_u32(D);
     constexpr uint32_t ID64 = tc::idesc_tf32(128, 64, 0, 0);
+    constexpr uint32_t IDZT = tc::idesc_tf32(128, 32, 0, 0);
+    // (ZT) Dz as [kz][b] and Ci as [b][kz] after the 2-D tables
+    const uint32_t sZt = tc::smem_u32(tab + Lay::kTableBytes), sCi = sZt + (uint32_t)(G * G * 4);
     constexpr uint32_t IDZ = tc::idesc_tf32(128, NT, 0, 0);
     uint64_t *mb = &mbar[wg];
     uint32_t phase = 0;
@@ -327,10 +375,13 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     // aligned 16-byte copies and the blocks are cut out of shared memory, and the aggregation adds
     // into a box before one pass of vector atomics.  Otherwise blocks are copied and added one by
     // one.  Every thread of the team calls bound_tile at the same point (it holds a team barrier).
+    // tiles: all of them, or those of a list (a.tlist, *a.tlist_n entries)
+    const long long nlist = a.tlist ? (long long)*a.tlist_n : ntiles;
     auto fetch_tile = [&](long long tl) {
         Tile T;
-        const long long grp = tl * GPT + wsub;
-        const bool inrange = tl < ntiles && grp < a.ngroups;
+        const long long tid = a.tlist ? (tl < nlist ? (long long)a.tlist[tl] : ntiles) : tl;
+        const long long grp = tid * GPT + wsub;
+        const bool inrange = tid < ntiles && grp < a.ngroups;
         T.g0 = inrange ? grp : 0;
         const int cnt = inrange ? a.count[T.g0] : 0;
         // full groups are filtered here; with kShort every group, block j if j < its count
@@ -414,7 +465,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     bound_tile(cur);
     if constexpr (Shp::kBoxes == 3)
         if (cur.region && pfirst < 3) load_boxes(cur, pfirst);
-    for (long long tile = (long long)blockIdx.x * NWG + wg; tile < ntiles && !failed; tile += tstride) {
+    for (long long tile = (long long)blockIdx.x * NWG + wg; tile < nlist && !failed; tile += tstride) {
         // the next tile's bounds (and, in the three-box form, its first boxes) are taken during
         // the gather of this tile's last plane
         Tile nxt = fetch_tile(tile + tstride);       // loads in flight during this tile
@@ -661,7 +712,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 }
             }
             // (Wiener) the group's levels, read before the shrinkage reuses the scratch row
-            if constexpr (WIENER) {
+            if constexpr (WIENER && !ZT) {
                 my_mu = part[r];
                 my_mur = part[128 + r];
             }
@@ -678,6 +729,111 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 tc::mma_commit(mb);
             }
             if (!wait_mma()) { failed = true; break; }
+            float denW = 0.0f, numW = 0.0f;
+            float s00 = 0.0f;                          // (old z stage) this row's shrunk (0, 0) coefficient
+            if constexpr (ZT) {
+                // 3'. transpose into the z-stage A operands: row (h, c) of Ys holds coefficient c of
+                // the blocks 64 h .. 64 h + 63 (K); Yr the same for the reference
+                const int rb = 64 * (r >> 6), kb = r & 63;
+#pragma unroll
+                for (int op = 0; op < 2; ++op) {
+                    float v[NC];
+#pragma unroll
+                    for (int q = 0; q < NC; q += 16) tc::tmem_ld16(tb + lrow + 64 * op + cb + q, *reinterpret_cast<float (*)[16]>(v + q));
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int e = 0; e < NC; ++e)
+                        *reinterpret_cast<float *>(D + op * Lay::kXBytes + tc::sw128_offset(rb + cb + e, kb, 128)) = v[e];
+                }
+                publish();
+                // 4'. z-DCT: lanes (h, c), columns 32 g' + kz of group g' of half h: the K range of
+                // the group's 32 blocks times Dz[kz][b] (source into cols 0-63, reference 64-127)
+                if (t == 0) {
+#pragma unroll 1
+                    for (int op = 0; op < 2; ++op)
+#pragma unroll 1
+                        for (int w2 = 0; w2 < 2; ++w2)
+#pragma unroll 1
+                            for (int s = 0; s < 4; ++s)
+                                tc::mma_ss_tf32(tb + 64 * op + 32 * w2,
+                                                tc::make_desc_sw128(sD + op * Lay::kXBytes + w2 * 16 * 1024 + s * 32, 1024),
+                                                tc::make_desc(sZt + s * 256, 128, 1024), IDZT, s > 0);
+                    tc::mma_commit(mb);
+                }
+                if (!wait_mma()) { failed = true; break; }
+                // 5'. Wiener shrinkage: thread (h, c) holds coefficient c of the 32 z frequencies of
+                // group g = 2 h + half, source and reference
+                {
+                    const int c = r & 63, g = 2 * (r >> 6) + half;
+                    float z[32], rr[32];
+                    tc::tmem_ld16(tb + lrow + cb, *reinterpret_cast<float (*)[16]>(z));
+                    tc::tmem_ld16(tb + lrow + cb + 16, *reinterpret_cast<float (*)[16]>(z + 16));
+                    tc::tmem_ld16(tb + lrow + 64 + cb, *reinterpret_cast<float (*)[16]>(rr));
+                    tc::tmem_ld16(tb + lrow + 64 + cb + 16, *reinterpret_cast<float (*)[16]>(rr + 16));
+                    tc::tmem_wait_ld();
+                    if (c == 0) {
+                        // the group's levels: (0, 0, 0) = 2 G sum (256 level) of the 2-D DC
+                        z[0] += part[32 * g] * (float)(512 * G);
+                        rr[0] += part[128 + 32 * g] * (float)(512 * G);
+                    }
+                    const float sg = a.wsig2[p][G - 1];
+                    float acc = 0.0f;
+#pragma unroll
+                    for (int e = 0; e < 32; ++e) {
+                        const float r2 = rr[e] * rr[e];
+                        const float w = __fdividef(r2, r2 + sg);
+                        z[e] *= w;
+                        acc = fmaf(w, w, acc);
+                    }
+                    if (c == 0) {
+                        // S(0, 0, 0) leaves the inverse products (added back per block, exactly)
+                        part[32 * g] = z[0];
+                        z[0] = 0.0f;
+                    }
+                    tc::tmem_st16(tb + lrow + cb, *reinterpret_cast<const float (*)[16]>(z));
+                    tc::tmem_st16(tb + lrow + cb + 16, *reinterpret_cast<const float (*)[16]>(z + 16));
+                    tc::tmem_wait_st();
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                    if (lane == 0) part[1 + 2 * g + ((r >> 5) & 1)] = acc;
+                }
+                publish();
+                // 6'. inverse z: T[(h, c)][32 g' + b] = sum_kz S[(h, c)][32 g' + kz] Ci[b][kz] (A from
+                // tensor memory) into cols 64-127
+                if (t == 0) {
+#pragma unroll 1
+                    for (int w2 = 0; w2 < 2; ++w2)
+#pragma unroll 1
+                        for (int s = 0; s < 4; ++s)
+                            tc::mma_ts_tf32(tb + 64 + 32 * w2, tb + 32 * w2 + 8 * s, tc::make_desc(sCi + s * 256, 128, 1024), IDZT, s > 0);
+                    tc::mma_commit(mb);
+                }
+                if (!wait_mma()) { failed = true; break; }
+                // T back to rows of blocks: At[b][c] (A operand of the inverse 2-D product)
+                {
+                    float v[NC];
+#pragma unroll
+                    for (int q = 0; q < NC; q += 16) tc::tmem_ld16(tb + lrow + 64 + cb + q, *reinterpret_cast<float (*)[16]>(v + q));
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int e = 0; e < NC; ++e)
+                        *reinterpret_cast<float *>(D + tc::sw128_offset(rb + cb + e, kb, 128)) = v[e];
+                }
+                publish();
+                if (t == 0) {
+                    xy_ss(0, sD, sKi);
+                    tc::mma_commit(mb);
+                }
+                if (!wait_mma()) { failed = true; break; }
+                // the block's group weights
+                {
+                    const int g = r / G;
+                    const float acc = part[1 + 2 * g] + part[2 + 2 * g];
+                    const float eps = 1.1920928955078125e-07f;
+                    denW = 1.0f / (acc > eps ? acc : eps);
+                    numW = denW / a.amp[G - 1];
+                }
+            } else {
             // 3. transpose into the z-stage B operand (reference rows below the source rows)
             row_to_column(0, 0, NT);
             if constexpr (WIENER) row_to_column(64, 64, NT);
@@ -821,7 +977,6 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             }
             // the shrunk (0, 0) coefficient of this row (Wiener: of the group's kz = 0 row) leaves
             // the inverse products
-            float s00 = 0.0f;
             if (cb == 0 && (!WIENER || j == 0)) {
                 float *s0p = reinterpret_cast<float *>(D + tc::sw128_offset(0, r, 64));
                 s00 = *s0p;
@@ -837,14 +992,13 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
             }
             if constexpr (!WIENER)
                 if (a.retained && mine && j == 0 && half == 0) a.retained[(long long)p * a.ngroups + g0] = (int)acc;
-            float denW;
             if constexpr (WIENER) {
                 const float eps = 1.1920928955078125e-07f;
                 denW = 1.0f / (acc > eps ? acc : eps);
             } else {
                 denW = acc < 1.0f ? 1.0f : 1.0f / acc;
             }
-            const float numW = denW / a.amp[gn - 1];
+            numW = denW / a.amp[gn - 1];
             publish();
             // (the barriers of the two inverse waits below order this before the aggregation)
             if constexpr (SPLIT >= 2) if (half == 0) part[r] = s00;
@@ -859,11 +1013,12 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 tc::mma_commit(mb);
             }
             if (!wait_mma()) { failed = true; break; }
+            }
             // 7. aggregation: rows -> shared memory (this quarter's 32 rows), then one block per step
             {
                 float v[NC];
 #pragma unroll
-                for (int c0 = 0; c0 < NC; c0 += 16) tc::tmem_ld16(tb + lrow + 64 + cb + c0, *reinterpret_cast<float (*)[16]>(v + c0));
+                for (int c0 = 0; c0 < NC; c0 += 16) tc::tmem_ld16(tb + lrow + (ZT ? 0 : 64) + cb + c0, *reinterpret_cast<float (*)[16]>(v + c0));
                 // the inverse of the (0, 0) coefficients: block j of the group gets
                 // sum_kz Ci[j][kz] S(kz, 0, 0), Ci[j][0] = 1, Ci[j][kz] = Dz[kz][j]
                 float dcb = 0.0f;
@@ -906,7 +1061,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 if constexpr (Shp::kBoxes == 3)
                     if (half == 0) rowtab[r].y = __float_as_int(numW);
                 int *Ri = reinterpret_cast<int *>(Rg);
-                if (Shp::kBoxes == 1 && region)           // (the three-box form clears it in the flush)
+                if ((Shp::kBoxes == 1 || ZT) && region)   // (the three-box form clears it in the flush)
                     for (int e = t; e < rh * rp; e += TEAM) Ri[e] = 0;
                 tc::wg_sync(bar_id, TEAM);
                 float scale = 1073741824.0f;                 // 2^30

@@ -932,7 +932,7 @@ public:
     DevBuf m_pos, m_n, m_key, v_pos, v_n, v_key;
     DevBuf d_sy, d_sx, scratch;
     DevBuf d_winb, d_winl, d_winc, d_slot0;
-    DevBuf tc_tab, tc_status, plist, plist_n;
+    DevBuf tc_tab, tc_status, plist, plist_n, tlists, tlist_n;
     // precision form, hard threshold: the recheck band (fraction of the threshold), the counters of
     // the last call ([0] coefficients recomputed in fp32, [1] decisions changed) and the retained-
     // coefficient count of every group of the last call ([plane][group])
@@ -981,6 +981,9 @@ public:
             // then the rows of the n-point z-stage matrices (Wiener kernels, tiles with short groups)
             std::vector<float> pt;
             cf_tc_partial_tables(para.G, pt);
+            ft.insert(ft.end(), pt.begin(), pt.end());
+            // then the transposed z stage's B operands
+            cf_tc_zt_tables(para.G, pt);
             ft.insert(ft.end(), pt.begin(), pt.end());
             const size_t fbase = img.size();
             img.resize(fbase + ft.size() * sizeof(float));
@@ -1251,6 +1254,22 @@ public:
             CU(cudaMemsetAsync(a.tc_stats, 0, 2 * sizeof(unsigned long long), stream));
             // precision form: full groups on the tensor cores, partial ones on the plain kernel
             // unless the tensor-core kernel takes them too (Wiener filter, G = 16 / 32)
+            if (cf_tc_zt_supported(para.B, para.G, wiener)) {
+                // tiles of full groups on the transposed z stage, tiles with a short group on the
+                // kernel with per-tile n-point matrices
+                const long long ntiles = (ngroups + 128 / para.G - 1) / (128 / para.G);
+                int *tl = static_cast<int *>(tlists.get(sizeof(int) * 2 * (size_t)std::max<long long>(1, ntiles)));
+                unsigned int *tn = static_cast<unsigned int *>(tlist_n.get(2 * sizeof(unsigned int)));
+                CU(cudaMemsetAsync(tn, 0, 2 * sizeof(unsigned int), stream));
+                CU(launch_cf_tile_lists(cnt, ngroups, para.G, tl, tn, tl + ntiles, tn + 1, stream));
+                a.tlist = tl;
+                a.tlist_n = tn;
+                CU(launch_cf_tc_zt(a, tc_tab.p, tc_status.as<int>(), stream));
+                a.tlist = tl + ntiles;
+                a.tlist_n = tn + 1;
+                CU(launch_cf_tc(a, tc_tab.p, tc_status.as<int>(), stream));
+                return;
+            }
             CU(launch_cf_tc(a, tc_tab.p, tc_status.as<int>(), stream));
             if (cf_tc_handles_partial(para.B, para.G, wiener)) return;
             a.skip_full = 1;

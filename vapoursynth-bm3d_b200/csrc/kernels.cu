@@ -271,15 +271,15 @@ void cf_tc_tables(int G, std::vector<unsigned char> &img)
     else tc_tables_t<32>(img);
 }
 
-template <int G, bool W>
+template <int G, bool W, bool ZT = false>
 static cudaError_t launch_cf_tc_t(const CFArgs &a, const void *tables, int *status, cudaStream_t s)
 {
-    using Shp = TcShape<G, W>;
+    using Shp = TcShape<G, W, ZT>;
     // 227 KB per CTA, less the kernel's 1 KB of static shared memory (barriers, aligned)
     static_assert(Shp::kSmem <= 232448 - 1024, "tensor-core filter: shared memory over the per-CTA limit");
     const size_t smem = (size_t)Shp::kSmem;
     cudaError_t e;
-    if ((e = allow_smem(cf_tc_kernel<G, W>, smem)) != cudaSuccess) return e;
+    if ((e = allow_smem(cf_tc_kernel<G, W, ZT>, smem)) != cudaSuccess) return e;
     int dev = 0, sms = 0;
     if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
     if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
@@ -287,8 +287,37 @@ static cudaError_t launch_cf_tc_t(const CFArgs &a, const void *tables, int *stat
     const long long ntiles = (a.ngroups + TcLayout<G>::kGroups - 1) / TcLayout<G>::kGroups;
     const long long grid = std::max<long long>(1, std::min<long long>((ntiles + Shp::kWG - 1) / Shp::kWG, sms));
     COUNT_LAUNCH();
-    cf_tc_kernel<G, W><<<(unsigned)grid, Shp::kTeam * Shp::kWG, smem, s>>>(a, static_cast<const float4 *>(tables), ntiles, status);
+    cf_tc_kernel<G, W, ZT><<<(unsigned)grid, Shp::kTeam * Shp::kWG, smem, s>>>(a, static_cast<const float4 *>(tables), ntiles, status);
     return cudaGetLastError();
+}
+
+int cf_tc_zt_supported(int B, int G, int wiener) { return B == 8 && G == 32 && wiener; }
+
+cudaError_t launch_cf_tile_lists(const int *count, long long ngroups, int G, int *full, unsigned int *nfull,
+                                 int *shrt, unsigned int *nshort, cudaStream_t s)
+{
+    const long long ntiles = (ngroups + 128 / G - 1) / (128 / G);
+    const long long blocks = std::max<long long>(1, std::min<long long>((ntiles + 255) / 256, 148LL * 8));
+    COUNT_LAUNCH();
+    cf_tile_lists_kernel<<<(unsigned)blocks, 256, 0, s>>>(count, ngroups, G, ntiles, full, nfull, shrt, nshort);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cf_tc_zt(const CFArgs &a, const void *tables, int *status, cudaStream_t s)
+{
+    if (!cf_tc_zt_supported(a.B, a.G, a.wiener)) return cudaErrorInvalidValue;
+    return launch_cf_tc_t<32, true, true>(a, tables, status, s);
+}
+
+// Dz as [kz][b] and Ci as [b][kz], K-major without swizzle (the transposed z stage's B operands)
+void cf_tc_zt_tables(int G, std::vector<float> &out)
+{
+    out.assign((size_t)2 * G * G, 0.0f);
+    for (int r = 0; r < G; ++r)
+        for (int k = 0; k < G; ++k) {
+            out[tc_kmajor(r, k, G) / 4] = round_tf32((float)cos2((long)(2 * k + 1) * r, 2L * G));
+            out[G * G + tc_kmajor(r, k, G) / 4] = round_tf32(k == 0 ? 1.0f : (float)cos2((long)k * (2 * r + 1), 2L * G));
+        }
 }
 
 cudaError_t launch_cf_tc(const CFArgs &a, const void *tables, int *status, cudaStream_t s)

@@ -63,6 +63,14 @@ void cf_tc_tables(int G, std::vector<unsigned char> &img);
 void cf_tc_partial_tables(int G, std::vector<float> &out);
 // 1 if the tensor-core kernel for (B, G, wiener) also filters the groups of fewer than G blocks
 int cf_tc_handles_partial(int B, int G, int wiener);
+// Transposed z stage (Wiener filter, B = 8, G = 32): the kernel for the tiles whose groups are all
+// full; launch_cf_tile_lists splits the tiles into those and the ones with a short group (device
+// lists and counts, counts zeroed by the caller), for a.tlist / a.tlist_n.
+int cf_tc_zt_supported(int B, int G, int wiener);
+void cf_tc_zt_tables(int G, std::vector<float> &out);
+cudaError_t launch_cf_tile_lists(const int *count, long long ngroups, int G, int *full, unsigned int *nfull,
+                                 int *shrt, unsigned int *nshort, cudaStream_t s);
+cudaError_t launch_cf_tc_zt(const CFArgs &a, const void *tables, int *status, cudaStream_t s);
 cudaError_t launch_cf_tc(const CFArgs &a, const void *tables, int *status, cudaStream_t s);
 
 // FP64 oracle of the collaborative filter, aggregation and normalisation for the groups of one

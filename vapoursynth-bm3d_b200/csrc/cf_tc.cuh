@@ -299,27 +299,32 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
         tc::wg_sync(bar_id, TEAM);
         tc::fence_after_sync();
     };
+    // Descriptor arithmetic: a descriptor's start address is in 16-byte units in its low bits, so
+    // the K steps of an operand are its first descriptor plus constants (the issue loops below are
+    // unrolled, so each product is one add and the instruction).
     // 2-D stage, A in shared memory: D[d0, +64) = X . K (X swizzled [128][64], K [64 n][64 k])
     auto xy_ss = [&](uint32_t d0, uint32_t sx, uint32_t sk) {
-#pragma unroll 1
+        const uint64_t ad = tc::make_desc_sw128(sx, 1024), bd = tc::make_desc(sk, 128, 2048);
+#pragma unroll
         for (int s = 0; s < 8; ++s)
-            tc::mma_ss_tf32(tb + d0, tc::make_desc_sw128(sx + (s / 4) * 16 * 1024 + (s % 4) * 32, 1024),
-                            tc::make_desc(sk + s * 256, 128, 2048), ID64, s > 0);
+            tc::mma_tf32_ss(tb + d0, ad + (uint64_t)(((s / 4) * 16 * 1024 + (s % 4) * 32) >> 4), bd + (uint64_t)(s * 16), ID64, s > 0);
     };
     // two independent 2-D products (source and reference) issued alternately
     auto xy_ss2 = [&](uint32_t d0, uint32_t sx, uint32_t d1, uint32_t sy, uint32_t sk) {
-#pragma unroll 1
+        const uint64_t ax = tc::make_desc_sw128(sx, 1024), ay = tc::make_desc_sw128(sy, 1024), bd = tc::make_desc(sk, 128, 2048);
+#pragma unroll
         for (int s = 0; s < 8; ++s) {
-            const uint64_t bd = tc::make_desc(sk + s * 256, 128, 2048);
-            tc::mma_ss_tf32(tb + d0, tc::make_desc_sw128(sx + (s / 4) * 16 * 1024 + (s % 4) * 32, 1024), bd, ID64, s > 0);
-            tc::mma_ss_tf32(tb + d1, tc::make_desc_sw128(sy + (s / 4) * 16 * 1024 + (s % 4) * 32, 1024), bd, ID64, s > 0);
+            const uint64_t ao = (uint64_t)(((s / 4) * 16 * 1024 + (s % 4) * 32) >> 4);
+            tc::mma_tf32_ss(tb + d0, ax + ao, bd + (uint64_t)(s * 16), ID64, s > 0);
+            tc::mma_tf32_ss(tb + d1, ay + ao, bd + (uint64_t)(s * 16), ID64, s > 0);
         }
     };
     // 2-D stage, A in tensor memory: D[d0, +64) = T[a0, +64) . K
     auto xy_ts = [&](uint32_t d0, uint32_t a0, uint32_t sk) {
-#pragma unroll 1
+        const uint64_t bd = tc::make_desc(sk, 128, 2048);
+#pragma unroll
         for (int s = 0; s < 8; ++s)
-            tc::mma_ts_tf32(tb + d0, tb + a0 + 8 * s, tc::make_desc(sk + s * 256, 128, 2048), ID64, s > 0);
+            tc::mma_tf32_ts(tb + d0, tb + a0 + 8 * s, bd + (uint64_t)(s * 16), ID64, s > 0);
     };
     // z stage: rows of group w of D[d0, +nt) = Zstack . Bt_w (K range of group w), every other
     // output lane disabled; Bt swizzled [nt rows][128 k]
@@ -749,15 +754,17 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 // 4'. z-DCT: lanes (h, c), columns 32 g' + kz of group g' of half h: the K range of
                 // the group's 32 blocks times Dz[kz][b] (source into cols 0-63, reference 64-127)
                 if (t == 0) {
-#pragma unroll 1
-                    for (int op = 0; op < 2; ++op)
-#pragma unroll 1
-                        for (int w2 = 0; w2 < 2; ++w2)
-#pragma unroll 1
-                            for (int s = 0; s < 4; ++s)
-                                tc::mma_ss_tf32(tb + 64 * op + 32 * w2,
-                                                tc::make_desc_sw128(sD + op * Lay::kXBytes + w2 * 16 * 1024 + s * 32, 1024),
-                                                tc::make_desc(sZt + s * 256, 128, 1024), IDZT, s > 0);
+                    // K step outer: consecutive products go to the four independent chains
+                    const uint64_t ad = tc::make_desc_sw128(sD, 1024), bd = tc::make_desc(sZt, 128, 1024);
+#pragma unroll
+                    for (int s = 0; s < 4; ++s)
+#pragma unroll
+                        for (int op = 0; op < 2; ++op)
+#pragma unroll
+                            for (int w2 = 0; w2 < 2; ++w2)
+                                tc::mma_tf32_ss(tb + 64 * op + 32 * w2,
+                                                ad + (uint64_t)((op * Lay::kXBytes + w2 * 16 * 1024 + s * 32) >> 4),
+                                                bd + (uint64_t)(s * 16), IDZT, s > 0);
                     tc::mma_commit(mb);
                 }
                 if (!wait_mma()) { failed = true; break; }
@@ -801,11 +808,12 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 // 6'. inverse z: T[(h, c)][32 g' + b] = sum_kz S[(h, c)][32 g' + kz] Ci[b][kz] (A from
                 // tensor memory) into cols 64-127
                 if (t == 0) {
-#pragma unroll 1
-                    for (int w2 = 0; w2 < 2; ++w2)
-#pragma unroll 1
-                        for (int s = 0; s < 4; ++s)
-                            tc::mma_ts_tf32(tb + 64 + 32 * w2, tb + 32 * w2 + 8 * s, tc::make_desc(sCi + s * 256, 128, 1024), IDZT, s > 0);
+                    const uint64_t bd = tc::make_desc(sCi, 128, 1024);
+#pragma unroll
+                    for (int s = 0; s < 4; ++s)
+#pragma unroll
+                        for (int w2 = 0; w2 < 2; ++w2)
+                            tc::mma_tf32_ts(tb + 64 + 32 * w2, tb + 32 * w2 + 8 * s, bd + (uint64_t)(s * 16), IDZT, s > 0);
                     tc::mma_commit(mb);
                 }
                 if (!wait_mma()) { failed = true; break; }

@@ -355,7 +355,8 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
             const float mg = (0.0009765625f * 1.01f + 1.52587890625e-05f) * sa * sb +
                              9.5367431640625e-07f * inv_s * (sa + sb) + 1.52587890625e-05f * (na + nbm);
             // pass 1: the K + 1 smallest upper bounds among candidates surely under the threshold
-            uint64_t b1 = ~0ull, b2 = ~0ull;
+            // (values only: two per lane, then the (K + 1)-th of the 64)
+            float f1 = 3.0e38f, f2 = 3.0e38f;
             int nsure = 0;
             for (int c0 = 0; c0 < ctot; c0 += 32) {
                 const int c = c0 + ((lane + 7 * (c0 >> 5)) & 31);
@@ -363,18 +364,19 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
                 const float hv = sd[c] + mg;
                 if (hv <= a.thSSE) {
                     ++nsure;
-                    const uint64_t v = compose(fmaxf(hv, 0.0f), (uint32_t)c);
-                    if (v < b1) { b2 = b1; b1 = v; } else if (v < b2) { b2 = v; }
+                    const float h = fmaxf(hv, 0.0f);
+                    f2 = fminf(f2, fmaxf(f1, h));
+                    f1 = fminf(f1, h);
                 }
             }
             nsure = warp_sum(nsure);
-            uint64_t v2[2] = {b1, b2};
-            warp_bitonic_u64<2>(v2);
-            const uint64_t TK = __shfl_sync(0xffffffffu, v2[0], K);
+            float v2[2] = {f1, f2};
+            warp_bitonic_f32<2>(v2);
+            const float TK = __shfl_sync(0xffffffffu, v2[0], K);
             // bound: the first K + 1 exact distances are <= bnd (K + 1 candidates have upper bounds
             // there), everything whose lower bound lies above it is settled
             const bool complete = nsure <= K;               // then every possibly valid candidate is listed
-            const float bnd = complete ? a.thSSE : fminf(a.thSSE, __uint_as_float((uint32_t)(TK >> 32)));
+            const float bnd = complete ? a.thSSE : fminf(a.thSSE, TK);
             // pass 2: the band of candidates whose lower bound is within it
             int ms = 0;
             const unsigned lt = (1u << lane) - 1u;

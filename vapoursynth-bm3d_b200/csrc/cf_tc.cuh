@@ -120,6 +120,10 @@ __host__ __device__ constexpr uint32_t tc_kmajor(int row, int k, int kdim)
 
 constexpr uint32_t kTcWaitLimit = 1u << 24;
 
+// floor(v / d) = umulhi(v, div_magic(d)) for 0 <= v < 2^16 and 1 <= d < 2^8: the magic number
+// exceeds 2^32 / d by less than 1, which moves v / d by less than 2^-16 < 1 / d
+__device__ __forceinline__ uint32_t div_magic(uint32_t d) { return 0xffffffffu / d + 1u; }
+
 // mean of the 64 pixels of a block held two per lane by a warp
 __device__ __forceinline__ float block_mean(float v0, float v1)
 {
@@ -440,9 +444,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     // source and reference boxes of plane pp of tile T (three-box form), as asynchronous copies
     auto load_boxes = [&](const Tile &T, int pp) {
         const long long fo = (long long)T.frame * a.frame_stride + (long long)T.y0 * a.ld + T.x0;
-        const int nv = T.rh * (T.rw >> 2);
+        const int w4 = T.rw >> 2, nv = T.rh * w4;
+        const uint32_t md = div_magic((uint32_t)w4);
         for (int v = t; v < nv; v += TEAM) {
-            const int yy = v / (T.rw >> 2), c4 = v - yy * (T.rw >> 2);
+            const int yy = (int)__umulhi((uint32_t)v, md), c4 = v - yy * w4;
             const long long go = fo + (long long)yy * a.ld + 4 * c4;
             tc::cp_async16(Bs + yy * T.rp + 4 * c4, a.src[pp] + go);
             tc::cp_async16(Br + yy * T.rp + 4 * c4, a.ref[pp] + go);
@@ -539,8 +544,11 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                             part[gfirst + k * G] = lv[2 * k];
                             part[128 + gfirst + k * G] = lv[2 * k + 1];
                         }
-                    // four block steps per round: their loads are issued before any store
-                    for (int i0 = half * NI; i0 < half * NI + NI; i0 += 4) {
+                    // four block steps per round: their loads are issued before any store (rounds
+                    // unrolled: the swizzle of each step's row is a constant)
+#pragma unroll
+                    for (int ii = 0; ii < NI; ii += 4) {
+                        const int i0 = half * NI + ii;
                         int pq[4];
                         float v0[4], v1[4], u0[4], u1[4];
 #pragma unroll
@@ -1087,7 +1095,9 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                 float *np = L.num + (long long)L.y * a.ld + L.x;
                 if (Shp::kBoxes == 3 && region) {
                     // four block steps per round: rows and table entries loaded before the atomics
-                    for (int i0 = half * NI; i0 < half * NI + NI; i0 += 4) {
+#pragma unroll
+                    for (int ii = 0; ii < NI; ii += 4) {
+                        const int i0 = half * NI + ii;
                         int2 q[4];
                         float x0v[4], x1v[4];
 #pragma unroll
@@ -1147,9 +1157,10 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                     // the region's sums, one vector atomic per 4 pixels (untouched ones skipped)
                     tc::wg_sync(bar_id, TEAM);
                     float *nbase = a.num[p] + (long long)frame * a.frame_stride + (long long)y0 * a.ld + x0;
-                    const int nv = rh * (rw >> 2);
+                    const int w4 = rw >> 2, nv = rh * w4;
+                    const uint32_t md = div_magic((uint32_t)w4);
                     for (int e = t; e < nv; e += TEAM) {
-                        const int yy = e / (rw >> 2), c4 = e - yy * (rw >> 2);
+                        const int yy = (int)__umulhi((uint32_t)e, md), c4 = e - yy * w4;
                         const int4 qi = *reinterpret_cast<const int4 *>(Ri + yy * rp + 4 * c4);
                         if (qi.x != 0 || qi.y != 0 || qi.z != 0 || qi.w != 0) {
                             const float inv = 1.0f / scale;

@@ -134,6 +134,38 @@ __device__ __forceinline__ void warp_bitonic_u64(uint64_t (&v)[V])
     }
 }
 
+// The same network over floats (values only).
+template <int V>
+__device__ __forceinline__ void warp_bitonic_f32(float (&v)[V])
+{
+    constexpr int M = 32 * V;
+    const int lane = (int)lane_id();
+#pragma unroll
+    for (int k = 2; k <= M; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+            for (int e = 0; e < V; ++e) {
+                const int i = e * 32 + lane;
+                const bool up = (i & k) == 0;
+                if (j >= 32) {
+                    const int pe = e ^ (j >> 5);
+                    if (pe > e) {
+                        const float a = v[e], b = v[pe];
+                        v[e] = up ? fminf(a, b) : fmaxf(a, b);
+                        v[pe] = up ? fmaxf(a, b) : fminf(a, b);
+                    }
+                } else {
+                    const float a = v[e];
+                    const float o = __shfl_xor_sync(0xffffffffu, a, j);
+                    const bool lower = (lane & j) == 0;
+                    v[e] = (lower == up) ? fminf(a, o) : fmaxf(a, o);
+                }
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ uint64_t compose(float positive_value, uint32_t idx)
 {
     return ((uint64_t)__float_as_uint(positive_value) << 32) | idx;

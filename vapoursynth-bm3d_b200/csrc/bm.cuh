@@ -258,6 +258,17 @@ __device__ __forceinline__ float exact_ssd8(const float *r, int rs, const float 
     return lane_combine(acc);
 }
 
+// exact_ssd8 with the reference block held as packed pairs rbp[y * 4 + m] = (r[y][2m], r[y][2m + 1])
+__device__ __forceinline__ float exact_ssd8_rb(const f32x2 (&rbp)[32], const float *w, int ws)
+{
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int y = 0; y < 8; ++y)
+#pragma unroll
+        for (int h = 0; h < 4; ++h) add_sq2(acc, h & 1, sub2(rbp[y * 4 + h], pack2(w[y * ws + 2 * h], w[y * ws + 2 * h + 1])));
+    return lane_combine(acc);
+}
+
 // Exact SSD (the reference's order) of the 8 x 8 reference block at rp (window, pitch wp) against
 // every lattice candidate (rows t + ry s, columns l + c s; window origin wy0, wx0) into
 // sd[ry * ncols + c], and against the trailing (0, 0) candidate of `plane` into sd[nrows * ncols].

@@ -389,7 +389,13 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
             }
             __syncwarp();
             if (ms <= 128) {
-                // exact distances of the band; invalid ones sort last
+                // exact distances of the band (the reference block in registers as packed pairs);
+                // invalid ones sort last
+                f32x2 rbp[32];
+#pragma unroll
+                for (int y = 0; y < 8; ++y)
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) rbp[y * 4 + m] = pack2(rp[y * L.wp + 2 * m], rp[y * L.wp + 2 * m + 1]);
                 uint64_t v[4] = {~0ull, ~0ull, ~0ull, ~0ull};
                 int nval = 0, nbelow = 0;
 #pragma unroll
@@ -397,7 +403,13 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
                     const int idx = lane + 32 * e;
                     if (idx < ms) {
                         const uint32_t c = list[idx];
-                        const float d = exact_of(c);
+                        float d;
+                        if ((int)c >= clat) {
+                            d = exact_of(c);
+                        } else {
+                            const int ry = (int)c / ncols, cc = (int)c - ry * ncols;
+                            d = exact_ssd8_rb(rbp, win + ry * L.wp + (l + cc - wx0), L.wp);
+                        }
                         if (dist_valid(d, a.thSSE)) {
                             v[e] = compose(d, c);
                             ++nval;
@@ -412,7 +424,8 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
                 // lies above bnd, so the band's first K + 1 are the first K + 1 overall (the last
                 // one decides whether the cut falls between equal keys).
                 if (complete || nbelow > K) {
-                    if (ms <= 64) warp_bitonic_u64<2>(*reinterpret_cast<uint64_t (*)[2]>(v));
+                    if (ms <= 32) warp_bitonic_u64<1>(*reinterpret_cast<uint64_t (*)[1]>(v));
+                    else if (ms <= 64) warp_bitonic_u64<2>(*reinterpret_cast<uint64_t (*)[2]>(v));
                     else warp_bitonic_u64<4>(v);
                     const int nout = min(nval, K);
                     // the reference's tie order only matters for equal keys: then fall back

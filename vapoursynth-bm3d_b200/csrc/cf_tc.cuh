@@ -791,15 +791,24 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                         z[0] += part[32 * g] * (float)(512 * G);
                         rr[0] += part[128 + 32 * g] * (float)(512 * G);
                     }
+                    // Wiener weights two coefficients at a time (packed fp32 pairs)
                     const float sg = a.wsig2[p][G - 1];
-                    float acc = 0.0f;
+                    const tc::f2 sg2 = tc::pk(sg, sg);
+                    tc::f2 acc2 = tc::pk(0.0f, 0.0f);
 #pragma unroll
-                    for (int e = 0; e < 32; ++e) {
-                        const float r2 = rr[e] * rr[e];
-                        const float w = __fdividef(r2, r2 + sg);
-                        z[e] *= w;
-                        acc = fmaf(w, w, acc);
+                    for (int e = 0; e < 32; e += 2) {
+                        const tc::f2 rv = tc::pk(rr[e], rr[e + 1]);
+                        const tc::f2 r2 = tc::mul2(rv, rv);
+                        const tc::f2 den = tc::fma2(rv, rv, sg2);
+                        float d0, d1;
+                        tc::upk(den, d0, d1);
+                        const tc::f2 w = tc::mul2(r2, tc::pk(__fdividef(1.0f, d0), __fdividef(1.0f, d1)));
+                        tc::upk(tc::mul2(tc::pk(z[e], z[e + 1]), w), z[e], z[e + 1]);
+                        acc2 = tc::fma2(w, w, acc2);
                     }
+                    float acc, acc_hi;
+                    tc::upk(acc2, acc, acc_hi);
+                    acc += acc_hi;
                     if (c == 0) {
                         // S(0, 0, 0) leaves the inverse products (added back per block, exactly)
                         part[32 * g] = z[0];

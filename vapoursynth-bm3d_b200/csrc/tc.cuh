@@ -190,6 +190,36 @@ __device__ __forceinline__ void cp_async_wait_all()
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// ---- packed pairs of fp32 values (sm_100 f32x2 arithmetic, each half an IEEE operation) -------
+
+typedef unsigned long long f2;
+
+__device__ __forceinline__ f2 pk(float lo, float hi)
+{
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+__device__ __forceinline__ void upk(f2 v, float &lo, float &hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+
+__device__ __forceinline__ f2 mul2(f2 a, f2 b)
+{
+    f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c)
+{
+    f2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+
 // ---- named barriers (one per tile team of threads) ---------------------------------------------------
 
 __device__ __forceinline__ void wg_sync(uint32_t id, uint32_t nthreads)

@@ -1175,7 +1175,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
                             const float inv = 1.0f / scale;
                             const float4 q = make_float4((float)qi.x * inv, (float)qi.y * inv, (float)qi.z * inv, (float)qi.w * inv);
                             atomicAdd(reinterpret_cast<float4 *>(nbase + (long long)yy * a.ld + 4 * c4), q);
-                            if constexpr (Shp::kBoxes == 3) *reinterpret_cast<int4 *>(Ri + yy * rp + 4 * c4) = make_int4(0, 0, 0, 0);
+                            // (the three-box form keeps its box zero; ZT zeroes it before each use)
+                            if constexpr (Shp::kBoxes == 3 && !ZT) *reinterpret_cast<int4 *>(Ri + yy * rp + 4 * c4) = make_int4(0, 0, 0, 0);
                         }
                     }
                 }

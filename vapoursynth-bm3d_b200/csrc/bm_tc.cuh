@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
     __shared__ float s_na[kBmtRefs];           // centred reference norms
     __shared__ int s_i[kBmtRefs], s_l[kBmtRefs], s_nc[kBmtRefs];   // column, first candidate column and count
     __shared__ int fail_flag;
+    __shared__ float z00[64];                  // the trailing candidate: the block at (0, 0) of the plane
 
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -118,6 +119,7 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
         float *dst = win + yy * L.wp;
         for (int xx = lane; xx < wcols; xx += 32) tc::cp_async4(dst + xx, src + xx);
     }
+    if (tid < 64) tc::cp_async4(&z00[tid], plane + (long long)(tid >> 3) * a.ld + (tid & 7));
     tc::cp_async_wait_all();
     tc::fence_before_sync();
     __syncthreads();
@@ -128,13 +130,13 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
     float cmean, sc, inv_s;
     {
         float s = 0.0f, lo = 3.0e38f, hi = -3.0e38f;
-        for (int e = tid; e < wrows * wcols; e += kBmtThreads) {
-            const int yy = e / wcols, xx = e - yy * wcols;
-            const float v = win[yy * L.wp + xx];
-            s += v;
-            lo = fminf(lo, v);
-            hi = fmaxf(hi, v);
-        }
+        for (int yy = warp; yy < wrows; yy += kBmtRefs)
+            for (int xx = lane; xx < wcols; xx += 32) {
+                const float v = win[yy * L.wp + xx];
+                s += v;
+                lo = fminf(lo, v);
+                hi = fmaxf(hi, v);
+            }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -333,7 +335,7 @@ __global__ void __launch_bounds__(kBmtThreads) bm_tc_kernel(BMArgs a, BmtLayout 
             return pack_yx(t + ry, l + cc);
         };
         auto exact_of = [&](uint32_t c) -> float {
-            if ((int)c >= clat) return exact_ssd8(rp, L.wp, plane, a.ld);
+            if ((int)c >= clat) return exact_ssd8(rp, L.wp, z00, 8);
             const int ry = (int)c / ncols, cc = (int)c - ry * ncols;
             return exact_ssd8(rp, L.wp, win + ry * L.wp + (l + cc - wx0), L.wp);
         };

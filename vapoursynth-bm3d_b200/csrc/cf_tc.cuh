@@ -373,7 +373,8 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     struct Tile {
         long long g0;
         uint32_t pk;
-        bool mine;
+        int cnt;                         // the row's group count (used a tile after its load)
+        bool inr;                        // the row's group exists
         bool region;
         int y0, x0, rh, rw, rp, frame;   // box origin, rows, width and shared-memory row pitch
     };
@@ -386,27 +387,29 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     // one.  Every thread of the team calls bound_tile at the same point (it holds a team barrier).
     // tiles: all of them, or those of a list (a.tlist, *a.tlist_n entries)
     const long long nlist = a.tlist ? (long long)*a.tlist_n : ntiles;
-    auto fetch_tile = [&](long long tl) {
+    // the tile id of list entry i, loaded a tile before the tile's own loads need it
+    auto tile_id = [&](long long i) -> long long { return a.tlist ? (i < nlist ? (long long)a.tlist[i] : ntiles) : i; };
+    auto fetch_tile = [&](long long tid) {
         Tile T;
-        const long long tid = a.tlist ? (tl < nlist ? (long long)a.tlist[tl] : ntiles) : tl;
         const long long grp = tid * GPT + wsub;
-        const bool inrange = tid < ntiles && grp < a.ngroups;
-        T.g0 = inrange ? grp : 0;
-        const int cnt = inrange ? a.count[T.g0] : 0;
-        // full groups are filtered here; with kShort every group, block j if j < its count
-        T.mine = inrange && (Shp::kShort ? j < cnt : cnt >= G);
+        T.inr = tid < ntiles && grp < a.ngroups;
+        T.g0 = T.inr ? grp : 0;
+        T.cnt = a.count[T.g0];
         T.pk = a.pos[T.g0 * G + j];
         T.region = false;
         T.y0 = T.x0 = T.rh = T.rw = T.rp = T.frame = 0;
         return T;
     };
+    // full groups are filtered here; with kShort every group, block j if j < its count
+    auto tile_mine = [&](const Tile &T) { return T.inr && (Shp::kShort ? j < T.cnt : T.cnt >= G); };
     auto bound_tile = [&](Tile &T) {
         if (!a.vbm3d) {
+            const bool tmine = tile_mine(T);
             const long long f = T.g0 / a.blocks_per_frame;
             const int py = unpack_y(T.pk), px = unpack_x(T.pk);
-            int ymin = T.mine ? py : 1 << 30, xmin = T.mine ? px : 1 << 30;
-            int ymax = T.mine ? py : -1, xmax = T.mine ? px : -1;
-            int fmin = T.mine ? (int)f : 1 << 30, fmax = T.mine ? (int)f : -1;
+            int ymin = tmine ? py : 1 << 30, xmin = tmine ? px : 1 << 30;
+            int ymax = tmine ? py : -1, xmax = tmine ? px : -1;
+            int fmin = tmine ? (int)f : 1 << 30, fmax = tmine ? (int)f : -1;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 ymin = min(ymin, __shfl_xor_sync(0xffffffffu, ymin, o));
@@ -471,16 +474,18 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     unsigned long long n_recheck = 0, n_changed = 0;
 
     bool failed = false;
-    Tile cur = fetch_tile((long long)blockIdx.x * NWG + wg);
+    Tile cur = fetch_tile(tile_id((long long)blockIdx.x * NWG + wg));
     bound_tile(cur);
+    long long nid = tile_id((long long)blockIdx.x * NWG + wg + tstride);
     if constexpr (Shp::kBoxes == 3)
         if (cur.region && pfirst < 3) load_boxes(cur, pfirst);
     for (long long tile = (long long)blockIdx.x * NWG + wg; tile < nlist && !failed; tile += tstride) {
         // the next tile's bounds (and, in the three-box form, its first boxes) are taken during
         // the gather of this tile's last plane
-        Tile nxt = fetch_tile(tile + tstride);       // loads in flight during this tile
+        Tile nxt = fetch_tile(nid);                  // loads in flight during this tile
+        nid = tile_id(tile + 2 * tstride);
         const long long g0 = cur.g0;
-        const bool mine = cur.mine;
+        const bool mine = tile_mine(cur);
         const uint32_t pk = cur.pk;
         const bool region = cur.region;
         const int y0 = cur.y0, x0 = cur.x0, rh = cur.rh, rw = cur.rw, rp = cur.rp, frame = cur.frame;

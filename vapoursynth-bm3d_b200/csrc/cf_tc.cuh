@@ -165,32 +165,92 @@ __device__ __forceinline__ void block_means(float (&s)[N], int lane)
     }
 }
 
-// Tiles (128 / G consecutive groups) split into those whose groups are all full and those with
-// a short group, each list in ascending order within a warp's 32 tiles.
-__global__ void cf_tile_lists_kernel(const int *__restrict__ count, long long ngroups, int G, long long ntiles,
-                                     int *__restrict__ full, unsigned int *__restrict__ nfull,
-                                     int *__restrict__ shrt, unsigned int *__restrict__ nshort)
+// Tiles (128 / G consecutive groups) split into those whose groups are all full and those with a
+// short group, both lists in ascending tile order (the persistent filter kernels walk them, and
+// neighbouring teams on neighbouring tiles keep the image rows and accumulators in L2).  Chunks of
+// kTileChunk tiles, one CTA each: the first kernel counts each chunk's full and short tiles, the
+// second adds the counts of the chunks before its own and writes its tiles at their ranks.
+constexpr int kTileChunk = 2048;             // 256 threads x 8 consecutive tiles
+
+__device__ __forceinline__ bool tile_full(const int *__restrict__ count, long long ngroups, int G, long long tl)
 {
-    const int lane = (int)(threadIdx.x & 31);
     const int gpt = 128 / G;
-    for (long long t0 = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); t0 < ntiles;
-         t0 += (long long)gridDim.x * blockDim.x) {
-        const long long tl = t0 + lane;
-        bool all = true;
-        if (tl < ntiles)
-            for (int k = 0; k < gpt; ++k) {
-                const long long g = tl * gpt + k;
-                if (g < ngroups && count[g] < G) all = false;
-            }
-#pragma unroll
-        for (int l = 0; l < 2; ++l) {
-            const bool in = tl < ntiles && (l == 0 ? all : !all);
-            const unsigned m = __ballot_sync(0xffffffffu, in);
-            unsigned base = 0;
-            if (lane == 0 && m) base = atomicAdd(l == 0 ? nfull : nshort, (unsigned)__popc(m));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (in) (l == 0 ? full : shrt)[base + __popc(m & ((1u << lane) - 1u))] = (int)tl;
-        }
+    bool all = true;
+    for (int k = 0; k < gpt; ++k) {
+        const long long g = tl * gpt + k;
+        if (g < ngroups && count[g] < G) all = false;
+    }
+    return all;
+}
+
+__global__ void __launch_bounds__(256) cf_tile_count_kernel(const int *__restrict__ count, long long ngroups, int G,
+                                                            long long ntiles, int *__restrict__ chunk_counts)
+{
+    __shared__ int sf[8], ss[8];
+    const long long base = (long long)blockIdx.x * kTileChunk + threadIdx.x * 8;
+    int nf = 0, ns = 0;
+    for (int k = 0; k < 8; ++k) {
+        const long long tl = base + k;
+        if (tl >= ntiles) break;
+        if (tile_full(count, ngroups, G, tl)) ++nf; else ++ns;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        nf += __shfl_xor_sync(0xffffffffu, nf, o);
+        ns += __shfl_xor_sync(0xffffffffu, ns, o);
+    }
+    if ((threadIdx.x & 31) == 0) { sf[threadIdx.x >> 5] = nf; ss[threadIdx.x >> 5] = ns; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int tf = 0, ts = 0;
+        for (int w = 0; w < 8; ++w) { tf += sf[w]; ts += ss[w]; }
+        chunk_counts[2 * blockIdx.x] = tf;
+        chunk_counts[2 * blockIdx.x + 1] = ts;
+    }
+}
+
+__global__ void __launch_bounds__(256) cf_tile_lists_kernel(const int *__restrict__ count, long long ngroups, int G,
+                                                            long long ntiles, const int *__restrict__ chunk_counts,
+                                                            int *__restrict__ full, unsigned int *__restrict__ nfull,
+                                                            int *__restrict__ shrt, unsigned int *__restrict__ nshort)
+{
+    __shared__ int sf[8], ss[8], bf, bs;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    // the chunk's first ranks: the counts of the chunks before it
+    int pf = 0, ps = 0;
+    for (int c = t; c < (int)blockIdx.x; c += 256) { pf += chunk_counts[2 * c]; ps += chunk_counts[2 * c + 1]; }
+    const long long base = (long long)blockIdx.x * kTileChunk + t * 8;
+    unsigned fm = 0;                         // bit k: tile base + k is full
+    int nf = 0, ns = 0;
+    for (int k = 0; k < 8; ++k) {
+        const long long tl = base + k;
+        if (tl >= ntiles) break;
+        if (tile_full(count, ngroups, G, tl)) { fm |= 1u << k; ++nf; } else { ++ns; }
+    }
+    // exclusive prefix of (nf, ns) over the CTA's threads, in thread order
+    int xf = nf, xs = ns;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int yf = __shfl_up_sync(0xffffffffu, xf, o), ys = __shfl_up_sync(0xffffffffu, xs, o);
+        if (lane >= o) { xf += yf; xs += ys; }
+    }
+    for (int o = 16; o > 0; o >>= 1) { pf += __shfl_xor_sync(0xffffffffu, pf, o); ps += __shfl_xor_sync(0xffffffffu, ps, o); }
+    if (lane == 31) { sf[w] = xf; ss[w] = xs; }
+    if (t == 0) { bf = 0; bs = 0; }
+    __syncthreads();
+    if (lane == 0) { atomicAdd(&bf, pf); atomicAdd(&bs, ps); }
+    int wf = 0, ws = 0;
+    for (int k = 0; k < w; ++k) { wf += sf[k]; ws += ss[k]; }
+    __syncthreads();
+    int of = bf + wf + xf - nf, os = bs + ws + xs - ns;
+    for (int k = 0; k < 8; ++k) {
+        const long long tl = base + k;
+        if (tl >= ntiles) break;
+        if (fm >> k & 1u) full[of++] = (int)tl; else shrt[os++] = (int)tl;
+    }
+    if (blockIdx.x == gridDim.x - 1 && t == 255) {
+        int tf = 0, ts = 0;
+        for (int k = 0; k < 8; ++k) { tf += sf[k]; ts += ss[k]; }
+        *nfull = (unsigned)(bf + tf);
+        *nshort = (unsigned)(bs + ts);
     }
 }
 

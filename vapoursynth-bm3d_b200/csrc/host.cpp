@@ -1258,10 +1258,10 @@ public:
                 // tiles of full groups on the transposed z stage, tiles with a short group on the
                 // kernel with per-tile n-point matrices
                 const long long ntiles = (ngroups + 128 / para.G - 1) / (128 / para.G);
-                int *tl = static_cast<int *>(tlists.get(sizeof(int) * 2 * (size_t)std::max<long long>(1, ntiles)));
+                const long long nch = cf_tile_chunks(ngroups, para.G);
+                int *tl = static_cast<int *>(tlists.get(sizeof(int) * (2 * (size_t)std::max<long long>(1, ntiles) + 2 * (size_t)nch)));
                 unsigned int *tn = static_cast<unsigned int *>(tlist_n.get(2 * sizeof(unsigned int)));
-                CU(cudaMemsetAsync(tn, 0, 2 * sizeof(unsigned int), stream));
-                CU(launch_cf_tile_lists(cnt, ngroups, para.G, tl, tn, tl + ntiles, tn + 1, stream));
+                CU(launch_cf_tile_lists(cnt, ngroups, para.G, tl, tn, tl + ntiles, tn + 1, tl + 2 * ntiles, stream));
                 a.tlist = tl;
                 a.tlist_n = tn;
                 CU(launch_cf_tc_zt(a, tc_tab.p, tc_status.as<int>(), stream));

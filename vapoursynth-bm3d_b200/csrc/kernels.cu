@@ -294,13 +294,23 @@ static cudaError_t launch_cf_tc_t(const CFArgs &a, const void *tables, int *stat
 int cf_tc_zt_supported(int B, int G, int wiener) { return B == 8 && G == 32 && wiener; }
 
 cudaError_t launch_cf_tile_lists(const int *count, long long ngroups, int G, int *full, unsigned int *nfull,
-                                 int *shrt, unsigned int *nshort, cudaStream_t s)
+                                 int *shrt, unsigned int *nshort, int *chunk_counts, cudaStream_t s)
 {
     const long long ntiles = (ngroups + 128 / G - 1) / (128 / G);
-    const long long blocks = std::max<long long>(1, std::min<long long>((ntiles + 255) / 256, 148LL * 8));
+    const long long chunks = std::max<long long>(1, (ntiles + kTileChunk - 1) / kTileChunk);
     COUNT_LAUNCH();
-    cf_tile_lists_kernel<<<(unsigned)blocks, 256, 0, s>>>(count, ngroups, G, ntiles, full, nfull, shrt, nshort);
+    cf_tile_count_kernel<<<(unsigned)chunks, 256, 0, s>>>(count, ngroups, G, ntiles, chunk_counts);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    COUNT_LAUNCH();
+    cf_tile_lists_kernel<<<(unsigned)chunks, 256, 0, s>>>(count, ngroups, G, ntiles, chunk_counts, full, nfull, shrt, nshort);
     return cudaGetLastError();
+}
+
+long long cf_tile_chunks(long long ngroups, int G)
+{
+    const long long ntiles = (ngroups + 128 / G - 1) / (128 / G);
+    return std::max<long long>(1, (ntiles + kTileChunk - 1) / kTileChunk);
 }
 
 cudaError_t launch_cf_tc_zt(const CFArgs &a, const void *tables, int *status, cudaStream_t s)

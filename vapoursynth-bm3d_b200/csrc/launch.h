@@ -65,11 +65,12 @@ void cf_tc_partial_tables(int G, std::vector<float> &out);
 int cf_tc_handles_partial(int B, int G, int wiener);
 // Transposed z stage (Wiener filter, B = 8, G = 32): the kernel for the tiles whose groups are all
 // full; launch_cf_tile_lists splits the tiles into those and the ones with a short group (device
-// lists and counts, counts zeroed by the caller), for a.tlist / a.tlist_n.
+// lists in ascending order and their counts), for a.tlist / a.tlist_n.
 int cf_tc_zt_supported(int B, int G, int wiener);
 void cf_tc_zt_tables(int G, std::vector<float> &out);
 cudaError_t launch_cf_tile_lists(const int *count, long long ngroups, int G, int *full, unsigned int *nfull,
-                                 int *shrt, unsigned int *nshort, cudaStream_t s);
+                                 int *shrt, unsigned int *nshort, int *chunk_counts, cudaStream_t s);
+long long cf_tile_chunks(long long ngroups, int G);   // ints of chunk_counts = 2 x this
 cudaError_t launch_cf_tc_zt(const CFArgs &a, const void *tables, int *status, cudaStream_t s);
 cudaError_t launch_cf_tc(const CFArgs &a, const void *tables, int *status, cudaStream_t s);
 

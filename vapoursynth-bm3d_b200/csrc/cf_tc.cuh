@@ -36,6 +36,19 @@
 //      atomics, then one pass of vector atomics to the numerator plane), otherwise straight to the
 //      numerator plane (one 32-byte sector per block row and atomic instruction instead of 32
 //      scattered sectors); the block weight goes to the weight map as in the plain kernel.
+// The transposed form (ZT, Wiener filter with G = 32, tiles of full groups) replaces steps 3-6:
+//   3'. each thread writes its block row's coefficients as column b % 64 of row (b / 64, c) of a
+//      source and a reference A operand (K = the 64 blocks of half tile b / 64)
+//   4'. z-DCT with the coefficients on the lanes: per half tile and group, D[(h, c)][32 g' + kz] =
+//      sum_b Ys[(h, c)][32 g' + b] Dz[kz][b], an M = 128, N = 32 product per K step (B = Dz in
+//      shared memory): each product is the group's own transform, nothing is masked
+//   5'. Wiener shrinkage per thread on its coefficient's 32 z frequencies of source and reference;
+//      the shrunk values go back to tensor memory and the group sums of the squared weights are
+//      combined over the two warps of the half tile's coefficients
+//   6'. inverse z with A = S from tensor memory and B = Ci, then a transpose back to block rows
+//      (an A operand in shared memory) for the inverse 2-D product
+// The tiles are taken from a list (a.tlist) when one is given: the transposed form walks the
+// tiles of full groups and the masked form the tiles with a short group.
 // Every wait on the tensor cores is bounded; on time-out the warpgroup records the failure in
 // *status and stops; the CTA releases its tensor memory and returns.
 #pragma once

@@ -361,7 +361,7 @@ cf_tc_kernel(CFArgs a, const float4 *tables, long long ntiles, int *status)
     uint32_t phase = 0;
 
     // Only the issuing warp polls the mbarrier; the team's other warps sleep in the barrier that
-    // passes its verdict on, instead of taking issue slots from the other team with their polls.
+    // passes its result on, instead of taking issue slots from the other team with their polls.
     auto wait_mma = [&]() -> bool {
         bool ok = true;
         if (t < 32) ok = tc::mbar_wait_bounded(mb, phase, kTcWaitLimit);

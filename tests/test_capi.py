@@ -131,5 +131,9 @@ def test_first_error_wins_in_reference_order():
 def test_valid_arguments_without_gpu_fail_loudly():
     rc, err = create("Basic", input=clip(), profile="np")
     assert rc == capi.BM3D_ERR_CUDA, err
+    # every precision value passes the argument checks (and then needs the device)
+    for prec in ("fp32", "tf32", "tf32_match", "learned"):
+        rc, err = create("Final", input=clip(), ref=clip(), precision=prec)
+        assert rc == capi.BM3D_ERR_CUDA, (prec, err)
     with pytest.raises(bm3d_b200.Error):
         bm3d_b200.core.bm3d.Basic(bm3d_b200.source(__import__("numpy").zeros((1, 3, 48, 64), "float32"), "RGB"))
